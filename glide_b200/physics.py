@@ -1,0 +1,399 @@
+"""IcePhysics: the drop-in API of the SSA forward/adjoint hot path.
+
+Same constructor and methods as glide/physics.py:49-259
+(``set_geometry``, ``set_parameters``, ``forward``, ``adjoint``,
+``reset_solution``, ``get_surface``, ``get_velocities_cell_centered``) and the
+same loss helpers (glide/physics.py:262-411).  Arrays are accepted as NumPy
+arrays, torch tensors or anything ``numpy.asarray`` understands; results are
+torch CUDA tensors that are views into the persistent state (overwritten by
+the next call, as in the reference).
+
+Additions (keyword-only):
+  precision  "fp32" (the reference's arithmetic, default), "fp64", or
+             "mixed": FP64 state and fine-grid residual/norms with FP32
+             V-cycles as the correction solver (defect correction).
+  forward(tol=..., max_vcycles=...)  stop on |r|/|r0| <= tol, where |r|
+             combines r_u, r_v and FB(r_H, H-gamma) (glide/physics.py:176-198)
+             and r0 is the residual of the step's starting state.
+  forward(guess=(u, v))  start from a supplied velocity guess; the plain
+             cycle finishes the solve and the guess is dropped when the first
+             cycle fails to cut the residual by ``guess_min_reduction``.
+  settings   solver settings (``SolverSettings``); defaults = reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .grid import Grid
+from .solver import REFERENCE, SolverSettings, native_levels, restrict_parameters_to_hierarchy
+
+RHO_ICE = 917.0
+G = 9.81
+
+_PRECISIONS = {"fp32": torch.float32, "fp64": torch.float64, "mixed": torch.float64}
+
+
+def _as_tensor(x, dtype, device, shape=None):
+    if isinstance(x, torch.Tensor):
+        t = x.detach().to(device=device, dtype=dtype)
+    else:
+        t = torch.as_tensor(np.asarray(x), dtype=dtype, device=device)
+    if shape is not None and t.dim() > 0 and tuple(t.shape) != tuple(shape):
+        raise ValueError(f"expected shape {tuple(shape)}, got {tuple(t.shape)}")
+    return t
+
+
+class IcePhysics:
+    """GPU shallow-shelf ice-flow model (forward step + adjoint) on one B200."""
+
+    def __init__(self, ny, nx, dx, n_levels=5, n=3.0, eps_reg=1e-5, thklim=0.1, water_drag=1e-3, calving_rate=1.0,
+                 gl_sigmoid_c=0.1, gl_derivatives=False, *, precision="fp32", device=None,
+                 settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0):
+        if precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        if not torch.cuda.is_available():
+            raise N.NativeError("IcePhysics needs a CUDA device")
+        if ny % (2 ** (n_levels - 1)) or nx % (2 ** (n_levels - 1)):
+            raise ValueError("ny and nx must be divisible by 2**(n_levels-1)")
+        self.ny, self.nx, self.dx, self.n_levels = int(ny), int(nx), float(dx), int(n_levels)
+        self.n, self.eps_reg, self.thklim = float(n), float(eps_reg), float(thklim)
+        self.water_drag, self.calving_rate = float(water_drag), float(calving_rate)
+        self.gl_sigmoid_c, self.gl_derivatives = float(gl_sigmoid_c), bool(gl_derivatives)
+        self.precision = precision
+        self.settings = settings or SolverSettings()
+        self.batch = int(batch)
+        self.use_graphs = bool(use_graphs)
+        self.guess_min_reduction = float(guess_min_reduction)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.kernels = N.load()
+        self.dtype = _PRECISIONS[precision]
+        self._init_hierarchy()
+        self._graphs = {}
+        self.last_history = []
+        self.last_info = {}
+
+    # ------------------------------------------------------------------ setup
+    def _make(self, dtype):
+        g = Grid(self.ny, self.nx, self.dx, dt=1.0, n=self.n, eps_reg=self.eps_reg, water_drag=self.water_drag,
+                 calving_rate=self.calving_rate, gl_sigmoid_c=self.gl_sigmoid_c, gl_derivatives=self.gl_derivatives,
+                 dtype=dtype, device=self.device, nb=self.batch)
+        gs = [g]
+        return g, gs
+
+    def _init_hierarchy(self):
+        if self.precision == "mixed":
+            self.grid, _ = self._make(torch.float64)
+            self.grids = [self.grid]
+            self.grid32, gs32 = self._make(torch.float32)
+            for _ in range(self.n_levels - 1):
+                gs32.append(gs32[-1].spawn_child())
+            self.grids32 = gs32
+            self._solve_grids = gs32
+        else:
+            self.grid, gs = self._make(self.dtype)
+            for _ in range(self.n_levels - 1):
+                gs.append(gs[-1].spawn_child())
+            self.grids = gs
+            self.grid32 = None
+            self._solve_grids = gs
+        self._native, self._nlev = native_levels(self._solve_grids[0])
+
+    def _shape(self):
+        return (self.ny, self.nx) if self.batch == 1 else (self.batch, self.ny, self.nx)
+
+    def _all_levels(self):
+        return self.grids + (self.grids32 if self.grid32 is not None else [])
+
+    def _propagate_geometry_to_hierarchy(self):
+        from .kernels import restrict_cell_centered
+        for hier in ([self.grids] if self.grid32 is None else [self.grids32]):
+            for par, ch in zip(hier[:-1], hier[1:]):
+                restrict_cell_centered(par.bed, None, f_coarse=ch.bed)
+                restrict_cell_centered(par.H, None, f_coarse=ch.H)
+                restrict_cell_centered(par.H_prev, None, f_coarse=ch.H_prev)
+                ch.gamma.fill_(self.thklim)
+
+    def set_geometry(self, bed, thickness):
+        """Bed and ice thickness (glide/physics.py:82-99)."""
+        g = self.grid
+        g.bed.copy_(_as_tensor(bed, g.dtype, self.device, self._shape()))
+        g.H.copy_(_as_tensor(thickness, g.dtype, self.device, self._shape()))
+        g.H_prev.copy_(g.H)
+        g.gamma.fill_(self.thklim)
+        if self.grid32 is not None:
+            g32 = self.grid32
+            g32.bed.copy_(g.bed)
+            g32.H.copy_(g.H)
+            g32.H_prev.copy_(g.H_prev)
+            g32.gamma.fill_(self.thklim)
+        self._propagate_geometry_to_hierarchy()
+
+    def set_parameters(self, B=None, beta=None, smb=None):
+        """Rate factor, basal friction, surface mass balance (glide/physics.py:101-129)."""
+        g = self.grid
+        if B is not None:
+            Bt = _as_tensor(B, g.dtype, self.device)
+            if Bt.dim() == 0:
+                g.B.fill_(float(Bt))
+            else:
+                g.B.copy_(Bt.reshape(self._shape()))
+        if beta is not None:
+            g.beta.copy_(_as_tensor(beta, g.dtype, self.device, self._shape()))
+        if smb is not None:
+            g.smb.copy_(_as_tensor(smb, g.dtype, self.device, self._shape()))
+        if self.grid32 is not None:
+            for name in ("B", "beta", "smb", "bed", "H_prev"):
+                getattr(self.grid32, name).copy_(getattr(g, name))
+            restrict_parameters_to_hierarchy(self.grid32)
+        else:
+            restrict_parameters_to_hierarchy(self.grid)
+
+    # ------------------------------------------------------------------ cycles
+    def _set_dt(self, dt):
+        for g in self._all_levels():
+            g.dt = float(dt)
+        # dt is passed to the kernels by value: rebuild the level descriptors
+        self._native, self._nlev = native_levels(self._solve_grids[0])
+
+    def _cfg(self):
+        return self.settings.native(self.thklim)
+
+    def _vcycle_native(self):
+        cfg = self._cfg()
+        N.check(self.kernels.glide_fascd_vcycle(self._native, self._nlev, 0, 1, C.byref(cfg), N.stream_handle()),
+                "fascd_vcycle")
+
+    def _dc_step(self):
+        """Mixed precision: one FP32 FASCD cycle as the correction solver of the
+        FP64 problem.  r64 = F64(U64) - f64; f32 = F32(U32) - r64 with
+        U32 = fl32(U64); after the cycle U64 += fl64(U32 - w32)."""
+        g64, g32 = self.grid, self.grid32
+        lib = self.kernels
+        s = N.stream_handle()
+        g64.compute_residual()
+        n = g64.nb * g64.n_total
+        N.check(lib.glide_convert(N.F32, g32.U.data_ptr(), g64.U.data_ptr(), n, 0, s), "convert")
+        N.check(lib.glide_convert(N.F32, g32.r.data_ptr(), g64.r.data_ptr(), n, 0, s), "convert")
+        a = g32.level_args()
+        N.check(lib.glide_residual(C.byref(a), g32.r_u.data_ptr(), g32.r_v.data_ptr(), g32.r_H.data_ptr(),
+                                   g32.f_u.data_ptr(), g32.f_v.data_ptr(), g32.f_H.data_ptr(), s), "residual32")
+        self._vcycle_native()   # sets w32 = U32 first
+        N.check(lib.glide_lincomb(N.F32, g32.z.data_ptr(), g32.U.data_ptr(), 1.0, g32.w.data_ptr(), -1.0, n, s),
+                "lincomb")
+        N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.z.data_ptr(), n, 1, s), "convert")
+
+    def _cycle(self):
+        if self.precision == "mixed":
+            self._dc_step()
+        else:
+            self._vcycle_native()
+
+    def _run_cycle(self):
+        """One V-cycle (or defect-correction step), replayed from a CUDA graph."""
+        if not self.use_graphs:
+            self._cycle()
+            return
+        key = (float(self.grid.dt),)
+        gr = self._graphs.get(key)
+        if gr is None:
+            # capture on a side stream; the kernels allocate nothing
+            self._cycle()  # warm-up launch (also checks arguments)
+            torch.cuda.synchronize()
+            gr = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gr):
+                self._cycle()  # recorded, not executed
+            self._graphs[key] = gr
+            return  # the warm-up call already did this cycle's work
+        gr.replay()
+
+    def residual_norm(self):
+        """|r| of the finest level with gamma = thklim (glide/physics.py:176-186); FP64, host float."""
+        g = self.grid
+        g.compute_residual()
+        sq = g.residual_norms()
+        return math.sqrt(float(sq.sum().item()))
+
+    # ------------------------------------------------------------------ API
+    def forward(self, dt, n_vcycles=3, verbose=False, update_geometry=True, *, tol=None, max_vcycles=100,
+                guess=None, history=None):
+        """One implicit time step (glide/physics.py:141-209).
+
+        Without ``tol`` runs ``n_vcycles`` cycles like the reference.  With
+        ``tol`` runs cycles until |r|/|r0| <= tol (or ``max_vcycles``).
+        """
+        self._set_dt(dt)
+        g = self.grid
+        g.f_H.copy_(g.H_prev / g.dt + g.smb)
+        if self.grid32 is not None:
+            self.grid32.f_H.copy_(g.f_H)  # overwritten by the correction RHS, kept for API reads
+        track = tol is not None or verbose or history is not None or guess is not None
+        r0 = self.residual_norm() if track else None
+        hist = [1.0] if track else []
+        info = {"vcycles": 0, "guess_used": False, "fallback": False}
+        if verbose:
+            print(f"  Initial: |r| = {r0:.2e}")
+        if guess is not None:
+            saved = g.U.clone()
+            gu, gv = guess
+            g.u.copy_(_as_tensor(gu, g.dtype, self.device))
+            g.v.copy_(_as_tensor(gv, g.dtype, self.device))
+            info["guess_used"] = True
+        n_max = max_vcycles if tol is not None else n_vcycles
+        k = 0
+        while k < n_max:
+            self._run_cycle()
+            k += 1
+            if track:
+                r = self.residual_norm()
+                rel = r / r0 if r0 > 0 else 0.0
+                if guess is not None and k == 1 and info["guess_used"]:
+                    # judge the guess by the first cycle: it must cut |r| by guess_min_reduction
+                    if not (rel * self.guess_min_reduction <= 1.0) or not math.isfinite(rel):
+                        g.U.copy_(saved)
+                        info["fallback"] = True
+                        info["guess_used"] = False
+                        hist.append(float("nan"))
+                        continue
+                hist.append(rel)
+                if verbose:
+                    print(f"  V-cycle {k - 1}: |r|/|r0| = {rel:.2e}")
+                if tol is not None and rel <= tol:
+                    break
+        info["vcycles"] = k
+        info["rel_residual"] = hist[-1] if hist else None
+        self.last_history = hist
+        self.last_info = info
+        if history is not None:
+            history.extend(hist)
+        if update_geometry:
+            g.H_prev.copy_(g.H)
+            if self.grid32 is not None:
+                self.grid32.H_prev.copy_(g.H)
+        return g.u, g.v, g.H
+
+    def adjoint(self, dL_du, dL_dv, dL_dH, n_vcycles=2, *, tol=None, max_vcycles=100, exact=False):
+        """grad_beta of a loss through one implicit step (glide/physics.py:211-242).
+
+        ``exact=True`` uses the exact transpose at clamped boundary reads in
+        the VJP and the gradient (the reference drops some boundary terms).
+        With ``tol`` the adjoint cycles run until |f_adj - J^T lam| <= tol*|f_adj|.
+        """
+        st = self.settings
+        saved_exact = st.exact_adjoint
+        st.exact_adjoint = bool(exact)
+        try:
+            g = self.grid
+            g.f_adj_u.copy_(-_as_tensor(dL_du, g.dtype, self.device))
+            g.f_adj_v.copy_(-_as_tensor(dL_dv, g.dtype, self.device))
+            g.f_adj_H.copy_(-_as_tensor(dL_dH, g.dtype, self.device))
+            g.Lambda.zero_()
+            cfg = st.native(self.thklim)
+            f0 = None
+            n_max = max_vcycles if tol is not None else n_vcycles
+            for k in range(n_max):
+                if self.precision == "mixed":
+                    self._adjoint_dc_step(cfg)
+                else:
+                    N.check(self.kernels.glide_adjoint_vcycle(self._native, self._nlev, 0, C.byref(cfg),
+                                                              N.stream_handle()), "adjoint_vcycle")
+                if tol is not None:
+                    rel, f0 = self._adjoint_rel(f0)
+                    if rel <= tol:
+                        break
+            return g.compute_grad_beta(exact_boundary=exact)
+        finally:
+            st.exact_adjoint = saved_exact
+
+    def _adjoint_rel(self, f0):
+        g = self.grid
+        g.mask.zero_()
+        g.compute_adjoint_residual(self.settings.exact_adjoint)
+        r = torch.sqrt(torch.sum(g.r_adj.double() ** 2)).item()
+        if f0 is None:
+            f0 = torch.sqrt(torch.sum(g.f_adj.double() ** 2)).item()
+        return (r / f0 if f0 > 0 else 0.0), f0
+
+    def _adjoint_dc_step(self, cfg):
+        """Mixed precision adjoint: r64 = f_adj - J64^T lam64, FP32 adjoint
+        cycle on J32^T d = fl32(r64), lam64 += fl64(d)."""
+        g64, g32 = self.grid, self.grid32
+        lib = self.kernels
+        s = N.stream_handle()
+        n = g64.nb * g64.n_total
+        g64.mask.zero_()
+        g64.compute_adjoint_residual(self.settings.exact_adjoint)
+        N.check(lib.glide_convert(N.F32, g32.U.data_ptr(), g64.U.data_ptr(), n, 0, s), "convert")
+        N.check(lib.glide_convert(N.F32, g32.f_adj.data_ptr(), g64.r_adj.data_ptr(), n, 0, s), "convert")
+        g32.Lambda.zero_()
+        N.check(lib.glide_adjoint_vcycle(self._native, self._nlev, 0, C.byref(cfg), s), "adjoint_vcycle")
+        N.check(lib.glide_convert(N.F64, g64.Lambda.data_ptr(), g32.Lambda.data_ptr(), n, 1, s), "convert")
+
+    def reset_solution(self):
+        """glide/physics.py:244-248."""
+        g = self.grid
+        g.u.zero_()
+        g.v.zero_()
+        g.H.copy_(g.H_prev)
+
+    def get_surface(self):
+        """s = H + max(bed, -0.917 H) (glide/physics.py:250-253)."""
+        g = self.grid
+        return g.H + torch.maximum(g.bed, -RHO_ICE / 1000.0 * g.H)
+
+    def get_velocities_cell_centered(self):
+        """glide/physics.py:255-259."""
+        g = self.grid
+        return 0.5 * (g.u[..., 1:] + g.u[..., :-1]), 0.5 * (g.v[..., 1:, :] + g.v[..., :-1, :])
+
+    def release_graphs(self):
+        self._graphs.clear()
+
+
+# ---------------------------------------------------------------------------
+# loss helpers (glide/physics.py:262-411)
+# ---------------------------------------------------------------------------
+
+def _nan0(d):
+    return torch.where(torch.isnan(d), torch.zeros_like(d), d)
+
+
+def huber_loss(u, v, u_obs, v_obs, eps=10.0):
+    du, dv = _nan0(u - u_obs), _nan0(v - v_obs)
+    return torch.sqrt(du ** 2 + eps).mean() + torch.sqrt(dv ** 2 + eps).mean()
+
+
+def huber_grad(u, v, u_obs, v_obs, eps=10.0):
+    du, dv = _nan0(u - u_obs), _nan0(v - v_obs)
+    n = u.numel()
+    return du / torch.sqrt(du ** 2 + eps) / n, dv / torch.sqrt(dv ** 2 + eps) / n
+
+
+def abs_loss(u, v, u_obs, v_obs):
+    du, dv = _nan0(u.double() - u_obs.double()), _nan0(v.double() - v_obs.double())
+    return du.abs().mean() + dv.abs().mean()
+
+
+def abs_grad(u, v, u_obs, v_obs, eps=10.0):
+    du, dv = _nan0(u - u_obs), _nan0(v - v_obs)
+    n = u.numel()
+    return torch.sign(du) / n, torch.sign(dv) / n
+
+
+def tikhonov_regularization(field):
+    dx_ = field[:, 1:] - field[:, :-1]
+    dy_ = field[1:, :] - field[:-1, :]
+    loss = 0.5 * (torch.sum(dx_ ** 2) + torch.sum(dy_ ** 2))
+    grad = torch.zeros_like(field)
+    grad[:, 1:-1] -= field[:, 2:] - 2 * field[:, 1:-1] + field[:, :-2]
+    grad[:, 0] -= field[:, 1] - field[:, 0]
+    grad[:, -1] -= field[:, -2] - field[:, -1]
+    grad[1:-1, :] -= field[2:, :] - 2 * field[1:-1, :] + field[:-2, :]
+    grad[0, :] -= field[1, :] - field[0, :]
+    grad[-1, :] -= field[-2, :] - field[-1, :]
+    return float(loss), grad

@@ -1,0 +1,159 @@
+/*
+ * glide_b200 C ABI: the SSA forward/adjoint hot path of GLIDE on one B200.
+ *
+ * Plain C types only (device pointers, sizes, a cudaStream_t passed as
+ * void*).  Every function returns 0 on success, a negative GLIDE_E_* code for
+ * invalid arguments, or a positive CUDA error code from the launch.  Nothing
+ * here allocates device memory; the caller owns every buffer.
+ *
+ * Grid layout (MAC staggered, glide/grid.py:1-8 of the reference):
+ *   u  (ny, nx+1) on vertical faces, v (ny+1, nx) on horizontal faces,
+ *   H and cell parameters (ny, nx); a batch of nb problems is stored
+ *   back to back (problem b at offset b * field_size).
+ * dtype: GLIDE_F32 or GLIDE_F64 for every floating-point buffer of a call.
+ *
+ * Reference interfaces replaced (paths inside glide-ism/glide):
+ *   glide_residual       <- compute_residual  glide/cuda/residuals.cu:6-24
+ *   glide_jvp            <- compute_jvp       glide/cuda/residuals.cu:299-317
+ *   glide_vjp            <- compute_vjp       glide/cuda/residuals.cu:586-604
+ *   glide_grad_beta      <- compute_grad_beta glide/cuda/grad.cu:1-17
+ *   glide_vanka_sweeps   <- vanka_smooth / vanka_smooth_local glide/cuda/vanka.cu:3-23,844-864
+ *                           + Grid.vanka_sweep(_local) glide/grid.py:305-317
+ *   glide_error_mask     <- error indicator of glide/solver.py:147-154
+ *   glide_vanka_adjoint  <- vanka_smooth_adjoint glide/cuda/vanka.cu:441-464
+ *   glide_restrict / glide_prolong <- restrict_* / prolongate_* glide/cuda/utility.cu:1-337,
+ *                           wrappers glide/kernels.py:90-236
+ *   glide_fascd_vcycle   <- fascd_vcycle   glide/solver.py:71-157
+ *   glide_adjoint_vcycle <- adjoint_vcycle glide/solver.py:160-220
+ *   GlidePhysicsParams   <- PhysicsParams  glide/cuda/common.cu:240-247 (same fields, double precision)
+ */
+#ifndef GLIDE_B200_H
+#define GLIDE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GLIDE_F32 0
+#define GLIDE_F64 1
+
+#define GLIDE_OK 0
+#define GLIDE_E_DTYPE (-1)
+#define GLIDE_E_SHAPE (-2)
+#define GLIDE_E_NULL (-3)
+#define GLIDE_E_GRAPH (-4)
+
+typedef struct GlidePhysicsParams {
+    double n;             /* Glen exponent */
+    double eps_reg;       /* strain-rate regularisation */
+    double water_drag;    /* drag under floating ice */
+    double calving_rate;
+    double gl_sigmoid_c;  /* grounding-line sigmoid sharpness */
+    int gl_derivatives;   /* include dH terms through the grounding sigmoid */
+} GlidePhysicsParams;
+
+/* One level (or a batch of equal-sized levels) and its state/parameters. */
+typedef struct GlideLevelArgs {
+    int ny, nx, nb, dtype;
+    double dx, dt;
+    GlidePhysicsParams params;
+    const void *u, *v, *H;               /* state; written by the smoothers */
+    const void *bed, *B, *beta;          /* cell parameters */
+    const void *mask, *gamma;            /* active-set mask and thickness limit, cells */
+} GlideLevelArgs;
+
+/* r = F(U) - f with the active-set row (1-m) r_H + m (H - gamma). */
+int glide_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, void* r_u, void* r_v,
+                   void* r_H, void* stream);
+/* J(U) d. */
+int glide_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const void* d_H, void* j_u, void* j_v,
+              void* j_H, void* stream);
+/* lambda^T J(U); with f_u/f_v/f_H non-null writes f - lambda^T J instead.
+ * exact_boundary = 0 reproduces the reference's boundary handling. */
+int glide_vjp(const GlideLevelArgs* a, const void* l_u, const void* l_v, const void* l_H, const void* f_u,
+              const void* f_v, const void* f_H, void* o_u, void* o_v, void* o_H, int exact_boundary, void* stream);
+/* grad_beta[c] = sum_faces lambda_face d tau_b / d beta_c (overwrites grad). */
+int glide_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, void* grad, int exact_boundary,
+                    void* stream);
+/* n_iter Vanka sweeps, each U += omega * delta (u, v, H of a updated in place).
+ * shift: diagonal shift of the local Newton matrix (reference: 1.0).
+ * flags/any_active non-null: local sweep gated by glide_error_mask's flags.
+ * scratch: 5 * ny * nx * nb elements of dtype. */
+int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
+                       int n_newton, double omega, double shift, const int* flags, const int* any_active,
+                       void* scratch, void* stream);
+/* err_mask = (|r_u|+|r_u|+|r_v|+|r_v|+|FB(r_H,H-gamma)| > threshold); if flags
+ * is non-null also the per-reference-block flags ((ny/14+1)*(nx/14+1)*nb ints)
+ * and any_active (nb ints). */
+int glide_error_mask(const GlideLevelArgs* a, const void* r_u, const void* r_v, const void* r_H, double threshold,
+                     void* err_mask, int* flags, int* any_active, void* stream);
+/* Block flags from an existing error mask. */
+int glide_tile_flags(const GlideLevelArgs* a, const void* err_mask, int* flags, int* any_active, void* stream);
+/* One colour of the red-black adjoint Vanka; lambda updated in place. */
+int glide_vanka_adjoint(const GlideLevelArgs* a, void* l_u, void* l_v, void* l_H, const void* ra_u, const void* ra_v,
+                        const void* ra_H, int color, double omega, void* stream);
+
+/* Transfers.  field: 0 = u faces, 1 = v faces, 2 = cells; sizes of the coarse grid. */
+int glide_restrict(int dtype, int field, int use_max, const void* fine, void* coarse, int nyc, int nxc, int nb,
+                   void* stream);
+int glide_prolong(int dtype, int field, int smooth, int add, const void* coarse, void* fine, int nyc, int nxc, int nb,
+                  void* stream);
+/* out = a*x + b*y (y may be null), n elements. */
+int glide_lincomb(int dtype, void* out, const void* x, double a, const void* y, double b, int64_t n, void* stream);
+int glide_fill(int dtype, void* out, double val, int64_t n, void* stream);
+/* mask = H <= gamma + tol */
+int glide_mask_le(int dtype, void* mask, const void* H, const void* gamma, double tol, int64_t n, void* stream);
+/* Convert between f32 and f64 buffers (out dtype = dst_dtype); out = x (+ add_to_out ? out : 0). */
+int glide_convert(int dst_dtype, void* out, const void* x, int64_t n, int accumulate, void* stream);
+/* Sums of squares of r_u, r_v, FB(r_H, H-gamma) into out3 (device double[3]);
+ * parts: glide_norm_parts(n) * 3 doubles of scratch.  Deterministic. */
+int glide_norms(int dtype, double* out3, double* parts, const void* r_u, const void* r_v, const void* r_H,
+                const void* H, const void* gamma, int64_t nu, int64_t nv, int64_t nc, void* stream);
+int glide_norm_parts(int64_t n);
+
+/* ---- multigrid driver ------------------------------------------------------ */
+/* Buffers of one level; U = [u|v|H] monolithic, likewise f, w, r, z, lam,
+ * f_adj, r_adj.  a.u/a.v/a.H must point into U. */
+typedef struct GlideLevel {
+    GlideLevelArgs a;
+    void *U, *f, *w, *r, *z;
+    void *chi, *err_mask;
+    void *lam, *f_adj, *r_adj;
+    void *H_prev, *smb;
+    void* scratch;          /* 5 * nc * nb */
+    int* flags;             /* (ny/14+1) * (nx/14+1) * nb */
+    int* any_active;        /* nb */
+} GlideLevel;
+
+typedef struct GlideSolverConfig {
+    double thklim;
+    int n_coarse, n_smooth, n_local_outer, n_local, n_newton;
+    double omega, shift, err_threshold;
+    int adj_coarse, adj_smooth;
+    double adj_omega;
+    int exact_adjoint;      /* 0: reference VJP boundary handling */
+} GlideSolverConfig;
+
+/* One FASCD V-cycle from level k0 (finest=1 sets w=U, chi=gamma-H first). */
+int glide_fascd_vcycle(GlideLevel* levels, int n_levels, int k0, int finest, const GlideSolverConfig* cfg,
+                       void* stream);
+int glide_adjoint_vcycle(GlideLevel* levels, int n_levels, int k0, const GlideSolverConfig* cfg, void* stream);
+/* restrict bed, B, beta, H_prev, smb from every level to its child (glide/solver.py:53-68) */
+int glide_restrict_parameters(GlideLevel* levels, int n_levels, int k0, void* stream);
+
+/* CUDA graphs of whole V-cycles.  kind: 0 = FASCD (finest), 1 = adjoint.
+ * The graph keeps the device pointers it was built with. */
+int glide_graph_create(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, int kind, void** graph_out);
+int glide_graph_launch(void* graph, void* stream);
+int glide_graph_destroy(void* graph);
+
+/* Library version string. */
+const char* glide_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

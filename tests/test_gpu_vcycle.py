@@ -1,0 +1,88 @@
+"""Solver parity: whole V-cycles and forward/adjoint steps vs the FP64 oracle.
+
+Tolerances: FP64 V-cycle state vs oracle <= 1e-8 relative (the cycle contains
+branch points such as the active-set switch and the error-mask threshold, so
+rounding-level differences of the operators can move a few values more than
+in a single operator); FP32 path vs FP64 path <= 2e-3 relative after two
+cycles of the reference settings.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _np(t):
+    return t.detach().double().cpu().numpy()
+
+
+def _case(n=32, levels=3):
+    from glide_b200.synthetic import dome_case
+    return dome_case(0, n=n, dx=5000.0 * 64 / n, n_levels=levels)
+
+
+def _physics(c, precision, **kw):
+    from glide_b200 import IcePhysics
+    ph = IcePhysics(c.ny, c.nx, c.dx, n_levels=c.n_levels, thklim=c.thklim, precision=precision, **kw)
+    ph.set_geometry(c.bed, c.thickness)
+    ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
+    return ph
+
+
+def _oracle(c, **kw):
+    from oracle.multigrid import OracleIcePhysics
+    ph = OracleIcePhysics(c.ny, c.nx, c.dx, n_levels=c.n_levels, thklim=c.thklim, **kw)
+    ph.set_geometry(c.bed, c.thickness)
+    ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
+    return ph
+
+
+def test_forward_fp64_vs_oracle():
+    c = _case()
+    ph = _physics(c, "fp64", use_graphs=False)
+    u, v, H = ph.forward(c.dt, n_vcycles=1)
+    ou, ov, oH = _oracle(c).forward(c.dt, n_vcycles=1)
+    assert _rel(_np(u), ou) <= 1e-8
+    assert _rel(_np(v), ov) <= 1e-8
+    assert _rel(_np(H), oH) <= 1e-8
+
+
+def test_forward_graph_matches_eager():
+    c = _case()
+    a = _physics(c, "fp64", use_graphs=False)
+    b = _physics(c, "fp64", use_graphs=True)
+    for _ in range(2):
+        ua, va, Ha = a.forward(c.dt, n_vcycles=2)
+        ub, vb, Hb = b.forward(c.dt, n_vcycles=2)
+    assert np.array_equal(_np(ua), _np(ub)) and np.array_equal(_np(Ha), _np(Hb))
+
+
+def test_forward_fp32_close_to_fp64():
+    c = _case()
+    a = _physics(c, "fp64")
+    b = _physics(c, "fp32")
+    ua, va, Ha = a.forward(c.dt, n_vcycles=2)
+    ub, vb, Hb = b.forward(c.dt, n_vcycles=2)
+    assert _rel(_np(ub), _np(ua)) <= 2e-3
+    assert _rel(_np(Hb), _np(Ha)) <= 2e-3
+
+
+def test_adjoint_fp64_vs_oracle():
+    c = _case()
+    ph = _physics(c, "fp64", use_graphs=False)
+    orc = _oracle(c)
+    ph.forward(c.dt, n_vcycles=1)
+    orc.forward(c.dt, n_vcycles=1)
+    rng = np.random.default_rng(3)
+    dLu = rng.standard_normal((c.ny, c.nx + 1)) * 1e-3
+    dLv = rng.standard_normal((c.ny + 1, c.nx)) * 1e-3
+    dLH = np.zeros((c.ny, c.nx))
+    g = ph.adjoint(dLu, dLv, dLH, n_vcycles=1)
+    og = orc.adjoint(dLu, dLv, dLH, n_vcycles=1)
+    assert _rel(_np(g), og) <= 1e-8
