@@ -144,16 +144,44 @@ def continental_case(seed=0):
     return ice_sheet_case(seed=seed, n=512, dx=1500.0, n_levels=5, name="continental512")
 
 
+def dome_sheet_case(seed=0, n=1024, dx=1000.0, n_levels=6, thklim=0.1, name=None):
+    """Grounded dome family (the config-1 geometry generalised to any size).
+
+    Paraboloid dome with a random centre offset (+-10% of the domain), radius
+    30-42% of the domain width and 1500-3000 m peak; bed = 3-6 Gaussian bumps
+    of +-500 m (width 1/10 of the domain) plus power-law noise (sigma 50 m);
+    log beta is a Gaussian random field (20 km correlation, sigma 0.5) around
+    log(1e3 Pa a/m); B = 1e8 Pa s^(1/3); SMB = 0.5 - 1e-3 (s - 1000) m/a.
+    """
+    rng = np.random.default_rng(seed)
+    Y, X = _centres(n, n, dx)
+    L = n * dx
+    cy, cx = rng.uniform(-0.1, 0.1, 2) * L
+    R = L * rng.uniform(0.30, 0.42)
+    hmax = rng.uniform(1500.0, 3000.0)
+    r2 = (X - cx) ** 2 + (Y - cy) ** 2
+    H = hmax * np.clip(1.0 - r2 / R ** 2, 0.0, None) + thklim
+    bed = _spectral_noise(rng, n, n, 50.0)
+    for _ in range(int(rng.integers(3, 7))):
+        by, bx = rng.uniform(-0.4, 0.4, 2) * L
+        amp = rng.uniform(-500.0, 500.0)
+        bed = bed + amp * np.exp(-((X - bx) ** 2 + (Y - by) ** 2) / (2 * (0.1 * L) ** 2))
+    logb = np.log(1e3) + 0.5 * _grf(rng, n, n, dx, 20e3)
+    beta = beta_head(np.exp(logb))
+    B = np.full((n, n), B_head(1e8))
+    smb = 0.5 - 1e-3 * (surface(bed, H) - 1000.0)
+    return Case(name or f"dome_sheet{n}", n, n, dx, n_levels, bed, H, B, beta, smb, dt=10.0, thklim=thklim,
+                info=dict(seed=seed, family="grounded dome", hmax=hmax, radius_m=R))
+
+
 def learned_guess_case(seed=0, n=1024, dx=1000.0, n_levels=6):
     """Fresh geometry for the learned-guess workload: 1024x1024, dx=1 km, 6 levels."""
-    return ice_sheet_case(seed=seed, n=n, dx=dx, n_levels=n_levels, name=f"sheet{n}")
+    return dome_sheet_case(seed=seed, n=n, dx=dx, n_levels=n_levels, name=f"sheet{n}")
 
 
 def training_patch_case(seed, n=256, dx=1000.0, n_levels=4):
-    """A 256x256 training patch (dx=1 km): a seeded ice sheet of random size."""
-    rng = np.random.default_rng(10_000 + seed)
-    return ice_sheet_case(seed=seed, n=n, dx=dx, n_levels=n_levels, h_max=float(rng.uniform(1500, 3500)),
-                          n_troughs=int(rng.integers(4, 12)), name=f"patch{n}")
+    """A 256x256 training patch (dx=1 km) from the same family."""
+    return dome_sheet_case(seed=10_000 + seed, n=n, dx=dx, n_levels=n_levels, name=f"patch{n}")
 
 
 def marine_case(seed=0, n=4096, dx=1000.0, n_levels=7, thklim=0.1):
