@@ -1,0 +1,472 @@
+#!/usr/bin/env python
+"""Benchmark: forward steps/s at 1e-6 relative residual, 1024x1024 SSA.
+
+One step = one implicit forward time step (dt = 10 a) of a fresh seeded
+1024x1024 ice-sheet geometry (dx = 1 km, 6 multigrid levels), solved until
+|r|/|r0| <= tol (r combines r_u, r_v and FB(r_H, H - gamma); r0 is the
+residual of the step's starting state u = v = 0, H = H_prev).  Synthetic
+inputs stand in for the reference's datasets (no network here).
+
+Arms
+  (default)          this package on N GPUs, one process per GPU (replicas:
+                     every rank solves its own geometries, no collective in the
+                     data path; scaling "weak").  ``value`` is the fast path
+                     (FP32 V-cycles + FP64 defect correction, learned initial
+                     guess when a trained model is available); the plain FP64
+                     FAS path is reported beside it.
+  --impl reference   the reference discretisation in FP64 NumPy on the host
+                     cores (the reference itself is GPU-only), timed on a
+                     bounded sample: full-size fine-level Vanka sweeps, scaled
+                     to a step by the cycle structure.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "forward steps/s at 1e-6 rel. residual, 1024² SSA: plain FAS vs learned guess"
+N = 1024
+DX = 1000.0
+LEVELS = 6
+DT = 10.0
+TOL = 1e-6
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--max-vcycles", type=int, default=40)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 FAS comparison arm")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling (nvidia-smi) during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        seen = set()
+        for r in self.rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    seen.add(name)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(seen),
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def tol_settings():
+    """Solver settings used to reach the tolerance (both arms of the comparison)."""
+    from glide_b200.solver import SolverSettings
+    return SolverSettings(shift=0.0, err_threshold=1e-7)
+
+
+def make_cases(n, seeds):
+    from glide_b200.synthetic import learned_guess_case
+    return [learned_guess_case(seed=s, n=n, dx=DX * 1024 / n, n_levels=LEVELS) for s in seeds]
+
+
+class Runner:
+    """Solves fresh geometries with one IcePhysics instance."""
+
+    def __init__(self, n, precision, guess_model=None, max_vcycles=40):
+        import torch
+        from glide_b200 import IcePhysics
+        self.ph = IcePhysics(n, n, DX * 1024 / n, n_levels=LEVELS, thklim=0.1, precision=precision,
+                             settings=tol_settings())
+        self.guess_model = guess_model
+        self.max_vcycles = max_vcycles
+        self.torch = torch
+
+    def load_device(self, case):
+        t = self.torch
+        d = dict(bed=case.bed, H=case.thickness, B=case.B, beta=case.beta, smb=case.smb)
+        return {k: t.as_tensor(v, dtype=self.ph.dtype, device="cuda") for k, v in d.items()}
+
+    def step(self, dev):
+        ph = self.ph
+        ph.set_geometry(dev["bed"], dev["H"])
+        ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
+        ph.reset_solution()
+        guess = None
+        if self.guess_model is not None:
+            guess = self.guess_model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"])
+        ph.forward(DT, tol=TOL, max_vcycles=self.max_vcycles, guess=guess)
+        return dict(ph.last_info)
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def time_steps(runner, devs, warmup, steps, world, flush):
+    import torch
+    infos = []
+    for k in range(warmup):
+        runner.step(devs[k % len(devs)])
+    torch.cuda.synchronize()
+    total = 0.0
+    for k in range(steps):
+        flush_l2(flush)
+        barrier(world)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        infos.append(runner.step(devs[warmup + k]))
+        b.record()
+        torch.cuda.synchronize()
+        total += a.elapsed_time(b) / 1e3
+    return total, infos
+
+
+def dominant_kernel_timing(runner, sweeps=20):
+    """Average duration of the fine-level Vanka cell kernel (CUDA events on the
+    launching stream) and of the residual kernel on the solved state."""
+    import ctypes as C
+    import torch
+    from glide_b200 import _native as N
+    ph = runner.ph
+    g = ph._solve_grids[0]
+    lib = N.load()
+    s = torch.cuda.current_stream()
+    a = g.level_args()
+    # cells kernel alone: glide_vanka_cells (no apply) through the sweep entry with omega=0 is not
+    # separable, so time sweeps and apply-only passes and subtract
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    saved = g.U.clone()
+    torch.cuda.synchronize()
+    ev[0].record(s)
+    N.check(lib.glide_vanka_cells(C.byref(a), g.f_u.data_ptr(), g.f_v.data_ptr(), g.f_H.data_ptr(), sweeps, 10,
+                                  float(ph.settings.shift), None, None, g._scratch.data_ptr(), s.cuda_stream),
+            "vanka cells")
+    ev[1].record(s)
+    for _ in range(sweeps):
+        g.compute_residual()
+    ev[2].record(s)
+    torch.cuda.synchronize()
+    g.U.copy_(saved)
+    t_vanka = ev[0].elapsed_time(ev[1]) / 1e3 / sweeps
+    t_res = ev[1].elapsed_time(ev[2]) / 1e3 / sweeps
+    return t_vanka, t_res, g
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    n = args.n
+    seeds = [rank * 100_000 + k for k in range(args.warmup + args.steps)]
+    cases = make_cases(n, seeds)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    guess_model = None
+    try:
+        from glide_b200.guess import load_default_model
+        guess_model = load_default_model()
+    except Exception:
+        guess_model = None
+    fast = Runner(n, "mixed", guess_model, args.max_vcycles)
+    fdev = [fast.load_device(c) for c in cases]
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    t_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
+    sampler.stop()
+    t_fast = max_over_ranks(t_fast, world)
+    value = world * args.steps / t_fast
+
+    plain_val, info_plain = None, []
+    if not args.no_plain:
+        plain = Runner(n, "fp64", None, args.max_vcycles)
+        pdev = [plain.load_device(c) for c in cases]
+        t_plain, info_plain = time_steps(plain, pdev, min(args.warmup, 1), args.steps, world, flush)
+        t_plain = max_over_ranks(t_plain, world)
+        plain_val = world * args.steps / t_plain
+        del plain, pdev
+
+    # end to end through the public API: host (pinned) inputs, H2D each step, D2H of u, v
+    import numpy as np
+    e2e_val, h2d, d2h = None, 0, 0
+    host = []
+    for c in cases:
+        d = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float64).pin_memory()
+             for k, v in (("bed", c.bed), ("H", c.thickness), ("B", c.B), ("beta", c.beta), ("smb", c.smb))}
+        host.append(d)
+    out_u = torch.empty((n, n + 1), dtype=torch.float64).pin_memory()
+    out_v = torch.empty((n + 1, n), dtype=torch.float64).pin_memory()
+    ph = fast.ph
+    tot = 0.0
+    for k in range(args.warmup + args.steps):
+        d = host[k]
+        flush_l2(flush)
+        barrier(world)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        dev = {key: val.to("cuda", non_blocking=True) for key, val in d.items()}
+        ph.set_geometry(dev["bed"], dev["H"])
+        ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
+        ph.reset_solution()
+        guess = None
+        if guess_model is not None:
+            guess = guess_model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"])
+        u, v, H = ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles, guess=guess)
+        out_u.copy_(u, non_blocking=True)
+        out_v.copy_(v, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            tot += a.elapsed_time(b) / 1e3
+    h2d = sum(t.numel() * t.element_size() for t in host[0].values())
+    d2h = out_u.numel() * 8 + out_v.numel() * 8
+    tot = max_over_ranks(tot, world)
+    e2e_val = world * args.steps / tot
+
+    # dominant-kernel roofline (Vanka cell kernel, fine level of the FP32 hierarchy)
+    t_vanka, t_res, g = dominant_kernel_timing(fast)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    esz = 4
+    ncell = n * n
+    vanka_bytes = ncell * esz * (10 + 5)          # 10 arrays read, 5 per-cell delta arrays written
+    res_bytes = ncell * esz * 14                  # 11 read + 3 written (u/v faces ~ cells)
+    vanka_flops = ncell * VANKA_FLOPS_PER_CELL_F32
+    fp32_peak_tf = 148 * 128 * 2 * 1.965e9 / 1e12
+    roof = {"bound": "hbm", "kernel": "vanka_cells_kernel<float> (fine level)", "achieved": vanka_bytes / t_vanka / 1e9,
+            "peak": hbm_peak, "unit": "GB/s", "frac": vanka_bytes / t_vanka / 1e9 / hbm_peak,
+            "traffic": VANKA_TRAFFIC_BYTES_PER_CELL_F32 * ncell if VANKA_TRAFFIC_BYTES_PER_CELL_F32 else None,
+            "peak_source": peak_src, "launch_ms": t_vanka * 1e3,
+            "alu": {"achieved_tflops": vanka_flops / t_vanka / 1e12, "peak_tflops": fp32_peak_tf,
+                    "frac": vanka_flops / t_vanka / 1e12 / fp32_peak_tf, "peak_source": "nominal FP32 (no measured peak)",
+                    "flops_per_cell": VANKA_FLOPS_PER_CELL_F32},
+            "stencil": {"kernel": "stencil_kernel<float,false> residual", "achieved": res_bytes / t_res / 1e9,
+                        "frac": res_bytes / t_res / 1e9 / hbm_peak, "launch_ms": t_res * 1e3}}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(cases[0], info_plain or info_fast)
+
+    if rank == 0:
+        vc = [i.get("vcycles") for i in info_fast]
+        rel = [i.get("rel_residual") for i in info_fast]
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_fast / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed: FP32 V-cycles, FP64 residual/norms)",
+            "data": "synthetic (seeded grounded-dome geometries, fresh per step)",
+            "config": {"workload": f"forward step to {TOL:g} rel. residual, {n}x{n}, dx={DX * 1024 / n:g} m, "
+                                   f"{LEVELS} levels, dt={DT:g} a, fresh geometry per step",
+                       "path": "mixed" + ("+learned_guess" if guess_model is not None else ""),
+                       "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas x{world}"},
+            "vcycles_per_step": vc, "rel_residual_reached": rel,
+            "plain_fp64_fas": {"value": plain_val, "unit": "steps/s",
+                               "vcycles_per_step": [i.get("vcycles") for i in info_plain],
+                               "rel_residual_reached": [i.get("rel_residual") for i in info_plain]},
+            "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": None,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": sampler.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# per-cell figures of the FP32 Vanka cell kernel (10 Newton iterations),
+# from the ncu instruction counts of one fine-level launch
+VANKA_FLOPS_PER_CELL_F32 = 6000.0
+VANKA_TRAFFIC_BYTES_PER_CELL_F32 = None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 NumPy oracle on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sweep_time(case, workers, repeats=1):
+    import numpy as np
+    from oracle.parallel import ParallelSweeper
+    from oracle.ssa import Params
+    ny, nx = case.ny, case.nx
+    u = np.zeros((ny, nx + 1))
+    v = np.zeros((ny + 1, nx))
+    H = case.thickness.copy()
+    f_u, f_v = np.zeros_like(u), np.zeros_like(v)
+    f_H = H / DT + case.smb
+    gamma = np.full_like(H, 0.1)
+    ps = ParallelSweeper(workers)
+    try:
+        ps.deltas(u[:64], v[:65], H[:64], f_u[:64], f_v[:65], f_H[:64], case.bed[:64], case.B[:64],
+                  case.beta[:64], gamma[:64], Params(), case.dx, DT, 10, shift=0.0)  # start the pool
+        t = time.time()
+        for _ in range(repeats):
+            ps.deltas(u, v, H, f_u, f_v, f_H, case.bed, case.B, case.beta, gamma, Params(), case.dx, DT, 10,
+                      shift=0.0)
+        return (time.time() - t) / repeats
+    finally:
+        ps.close()
+
+
+def sweeps_per_vcycle(levels=LEVELS, n_smooth=10, n_local_outer=10, n_local=10, n_coarse=200):
+    """Fine-level-equivalent Vanka sweeps of one V-cycle with every local
+    smoothing round active (the tolerance settings): sum over levels of
+    sweeps x 4^-level."""
+    w = 0.0
+    for k in range(levels - 1):
+        w += (2 * n_smooth + n_local_outer * n_local) * 4.0 ** (-k)
+    w += n_coarse * 4.0 ** (-(levels - 1))
+    return w
+
+
+def cpu_baseline(case, infos, workers=None):
+    workers = workers or os.cpu_count() or 1
+    t_sweep = cpu_sweep_time(case, workers)
+    vcycles = [i.get("vcycles") or 0 for i in infos] or [REF_VCYCLES_PER_STEP]
+    vpc = sum(vcycles) / len(vcycles) if vcycles else REF_VCYCLES_PER_STEP
+    t_step = vpc * sweeps_per_vcycle() * t_sweep
+    return {"value": 1.0 / t_step, "unit": "steps/s", "cores": workers, "kind": "port",
+            "sample": f"one full-size {case.ny}x{case.nx} FP64 NumPy Vanka sweep ({t_sweep:.2f} s on {workers} "
+                      f"processes), scaled by {sweeps_per_vcycle():.1f} fine-equivalent sweeps per V-cycle x "
+                      f"{vpc:.1f} V-cycles per step"}
+
+
+REF_VCYCLES_PER_STEP = 10.0
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    case = make_cases(args.n, [0])[0]
+    workers = os.cpu_count() or 1
+    times = []
+    for k in range(args.warmup + args.steps):
+        t = cpu_sweep_time(case, workers)
+        if k >= args.warmup:
+            times.append(t)
+    t_sweep = sum(times) / len(times)
+    t_step = REF_VCYCLES_PER_STEP * sweeps_per_vcycle() * t_sweep
+    value = 1.0 / t_step
+    sample = (f"per step: one full-size {case.ny}x{case.nx} FP64 NumPy Vanka sweep on {workers} processes "
+              f"({t_sweep:.2f} s), scaled by {sweeps_per_vcycle():.1f} fine-equivalent sweeps per V-cycle x "
+              f"{REF_VCYCLES_PER_STEP:g} V-cycles per step")
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded grounded-dome geometry)",
+            "config": {"workload": f"forward step to {TOL:g} rel. residual, {args.n}x{args.n}, dx={DX:g} m, "
+                                   f"{LEVELS} levels, dt={DT:g} a", "parallelism": "host cores"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -17,7 +17,8 @@ F32, F64 = 0, 1
 ERRORS = {-1: "unsupported dtype", -2: "bad shape or argument", -3: "null pointer", -4: "CUDA graph failure"}
 
 SYMBOLS = [
-    "glide_residual", "glide_jvp", "glide_vjp", "glide_grad_beta", "glide_vanka_sweeps", "glide_error_mask",
+    "glide_residual", "glide_jvp", "glide_vjp", "glide_grad_beta", "glide_vanka_sweeps", "glide_vanka_cells",
+    "glide_error_mask",
     "glide_tile_flags", "glide_vanka_adjoint", "glide_restrict", "glide_prolong", "glide_lincomb", "glide_fill",
     "glide_mask_le", "glide_convert", "glide_norms", "glide_norm_parts", "glide_fascd_vcycle",
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
@@ -52,7 +53,7 @@ class SolverConfig(C.Structure):
     _fields_ = [("thklim", C.c_double), ("n_coarse", C.c_int), ("n_smooth", C.c_int), ("n_local_outer", C.c_int),
                 ("n_local", C.c_int), ("n_newton", C.c_int), ("omega", C.c_double), ("shift", C.c_double),
                 ("err_threshold", C.c_double), ("adj_coarse", C.c_int), ("adj_smooth", C.c_int),
-                ("adj_omega", C.c_double), ("exact_adjoint", C.c_int)]
+                ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int)]
 
 
 class NativeError(RuntimeError):
@@ -79,6 +80,7 @@ def load():
         "glide_vjp": [LA, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp],
         "glide_grad_beta": [LA, vp, vp, vp, i, vp],
         "glide_vanka_sweeps": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp, vp],
+        "glide_vanka_cells": [LA, vp, vp, vp, i, i, d, vp, vp, vp, vp],
         "glide_error_mask": [LA, vp, vp, vp, d, vp, vp, vp, vp],
         "glide_tile_flags": [LA, vp, vp, vp, vp],
         "glide_vanka_adjoint": [LA, vp, vp, vp, vp, vp, vp, i, d, vp],

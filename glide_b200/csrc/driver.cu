@@ -16,6 +16,7 @@ template <typename T> int launch_jvp(const GlideLevelArgs*, const void*, const v
 template <typename T> int launch_vjp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*, void*, void*, void*, int, cudaStream_t);
 template <typename T> int launch_grad_beta(const GlideLevelArgs*, const void*, const void*, void*, int, cudaStream_t);
 template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t);
+template <typename T> int launch_vanka_cells(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, const int*, const int*, void*, cudaStream_t);
 template <typename T> int launch_error_mask(const GlideLevelArgs*, const void*, const void*, const void*, double, void*, int*, int*, cudaStream_t);
 template <typename T> int launch_tile_flags(const GlideLevelArgs*, const void*, int*, int*, cudaStream_t);
 template <typename T> int launch_vanka_adjoint(const GlideLevelArgs*, void*, void*, void*, const void*, const void*, const void*, int, double, cudaStream_t);
@@ -38,12 +39,6 @@ __global__ void convert_k(D* __restrict__ out, const S* __restrict__ x, int64_t 
 }  // namespace glide
 
 using namespace glide;
-
-#define DISPATCH(dt, ...)                                         \
-    do {                                                          \
-        if ((dt) == GLIDE_F32) return launch_##__VA_ARGS__;        \
-        if ((dt) == GLIDE_F64) return launch_##__VA_ARGS__;        \
-    } while (0)
 
 static inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
@@ -113,6 +108,21 @@ int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v
                                                 scratch, S(stream)),
                      launch_vanka_sweeps<double>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags,
                                                  any_active, scratch, S(stream)));
+}
+
+int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,
+                      int n_newton, double shift, const int* flags, const int* any_active, void* scratch,
+                      void* stream) {
+    int e = check_level(a);
+    if (e) return e;
+    if (!f_u || !f_v || !f_H || !scratch) return GLIDE_E_NULL;
+    if ((flags == nullptr) != (any_active == nullptr)) return GLIDE_E_NULL;
+    if (n_launch < 0 || n_newton < 0) return GLIDE_E_SHAPE;
+    return TDISPATCH(a->dtype,
+                     launch_vanka_cells<float>(a, f_u, f_v, f_H, n_launch, n_newton, shift, flags, any_active,
+                                               scratch, S(stream)),
+                     launch_vanka_cells<double>(a, f_u, f_v, f_H, n_launch, n_newton, shift, flags, any_active,
+                                                scratch, S(stream)));
 }
 
 int glide_error_mask(const GlideLevelArgs* a, const void* r_u, const void* r_v, const void* r_H, double threshold,
@@ -299,7 +309,7 @@ int fascd(GlideLevel* lv, int n, int k, bool finest, const GlideSolverConfig* c,
     TRY(glide_lincomb(wc.dt, C->z, C->U, 1.0, C->w, -1.0, wc.ntot * wc.nb, s));
     TRY(glide_prolong(w.dt, 0, 1, 1, wc.u(C->z), w.u(L->U), C->a.ny, C->a.nx, C->a.nb, s));
     TRY(glide_prolong(w.dt, 1, 1, 1, wc.v(C->z), w.v(L->U), C->a.ny, C->a.nx, C->a.nb, s));
-    TRY(glide_prolong(w.dt, 2, 0, 1, wc.H(C->z), w.H(L->U), C->a.ny, C->a.nx, C->a.nb, s));
+    TRY(glide_prolong(w.dt, 2, c->smooth_H_correction, 1, wc.H(C->z), w.H(L->U), C->a.ny, C->a.nx, C->a.nb, s));
     // post-smoothing and local error-driven smoothing   (solver.py:143-157)
     TRY(gamma_from(L, L->chi, s));
     TRY(vanka(L, c->n_smooth, c, false, s));

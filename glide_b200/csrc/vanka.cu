@@ -213,10 +213,210 @@ __device__ __forceinline__ bool ref_tile_on(const int* flags, int i, int j, int 
     return flags[(i / REF_STRIDE) * nbx + j / REF_STRIDE] != 0;
 }
 
+// Frozen per-cell coefficients of the forward local Newton loop: every term
+// that depends only on neighbour values (fixed during a cell's iterations) is
+// evaluated once here, so the loop only evaluates what depends on the cell's
+// own 5 unknowns.  Same formulas as assemble<T,true>; the neighbour normal
+// stresses are kept as k*(x - x_far) + c so no cancellation is introduced.
+template <typename T> struct Frozen {
+    T eta_c, ec;                       // eta of the cell, 0.25*eta
+    T kl, cl, u_ll, kr, cr, u_rr;      // sxx of left/right cell
+    T kt, ct, v_tt, kb, cb, v_bb;      // syy of top/bottom cell
+    T S_tl, S_tr, S_bl, S_br;          // 0.25 * sum of the 3 frozen eta*H around each vertex
+    T u_tl, v_lt, u_tr, v_rt, u_bl, v_lb, u_br, v_rb;
+    T w_tl, w_tr, w_bl, w_br;          // vertex validity (0/1)
+    T be_l, be_r, be_t, be_b;          // neighbour half of beta_eff: g*beta + (1-g)*wd
+    T g_l, g_r, g_t, g_b;              // neighbour grounded fractions (gl_derivatives only)
+    T beta_l, beta_r, beta_t, beta_b;
+    T H_l, H_r, H_t, H_b;
+    T S_l, S_r, S_t, S_b;              // neighbour surfaces max(bed,-0.917H)+H
+    T db_l, db_r, db_t, db_b;          // 1 + dbase/dH of the neighbours
+    T w_l, w_r, w_t, w_b;              // flux / driving validity of the 4 faces
+    T bed_c, beta_c;
+};
+
+template <typename T>
+__device__ __forceinline__ void make_frozen(Frozen<T>& F, const Patch<T>& P, int ny, int nx, const Phys<T>& p) {
+    const int i = P.i, j = P.j;
+    const T dxi = p.dxi;
+    const T (&eta)[3][3] = P.eta;
+    const T (&Hn)[3][3] = P.Hn;
+    F.eta_c = eta[1][1];
+    F.ec = T(0.25) * eta[1][1];
+    T wl = (j - 1 >= 0) ? T(1) : T(0), wr = (j + 1 < nx) ? T(1) : T(0);
+    T wt = (i - 1 >= 0) ? T(1) : T(0), wb = (i + 1 < ny) ? T(1) : T(0);
+    T eHl = eta[1][0] * Hn[1][0], eHr = eta[1][2] * Hn[1][2], eHt = eta[0][1] * Hn[0][1], eHb = eta[2][1] * Hn[2][1];
+    F.kl = T(4) * eHl * dxi * wl;  F.cl = T(2) * eHl * dxi * wl * (P.v_lt - P.v_lb);  F.u_ll = P.u_ll;
+    F.kr = T(4) * eHr * dxi * wr;  F.cr = T(2) * eHr * dxi * wr * (P.v_rt - P.v_rb);  F.u_rr = P.u_rr;
+    F.kt = T(4) * eHt * dxi * wt;  F.ct = T(2) * eHt * dxi * wt * (P.u_tr - P.u_tl);  F.v_tt = P.v_tt;
+    F.kb = T(4) * eHb * dxi * wb;  F.cb = T(2) * eHb * dxi * wb * (P.u_br - P.u_bl);  F.v_bb = P.v_bb;
+    F.S_tl = T(0.25) * (eta[0][0] * Hn[0][0] + eHt + eHl);
+    F.S_tr = T(0.25) * (eHt + eta[0][2] * Hn[0][2] + eHr);
+    F.S_bl = T(0.25) * (eHl + eta[2][0] * Hn[2][0] + eHb);
+    F.S_br = T(0.25) * (eHr + eHb + eta[2][2] * Hn[2][2]);
+    F.u_tl = P.u_tl; F.v_lt = P.v_lt; F.u_tr = P.u_tr; F.v_rt = P.v_rt;
+    F.u_bl = P.u_bl; F.v_lb = P.v_lb; F.u_br = P.u_br; F.v_rb = P.v_rb;
+    F.w_tl = (i > 0 && j > 0) ? T(1) : T(0);
+    F.w_tr = (i > 0 && j + 1 < nx) ? T(1) : T(0);
+    F.w_bl = (i + 1 < ny && j > 0) ? T(1) : T(0);
+    F.w_br = (i + 1 < ny && j + 1 < nx) ? T(1) : T(0);
+    F.g_l = P.g_l; F.g_r = P.g_r; F.g_t = P.g_t; F.g_b = P.g_b;
+    F.beta_l = P.beta_l; F.beta_r = P.beta_r; F.beta_t = P.beta_t; F.beta_b = P.beta_b;
+    F.be_l = P.g_l * P.beta_l + (T(1) - P.g_l) * p.water_drag;
+    F.be_r = P.g_r * P.beta_r + (T(1) - P.g_r) * p.water_drag;
+    F.be_t = P.g_t * P.beta_t + (T(1) - P.g_t) * p.water_drag;
+    F.be_b = P.g_b * P.beta_b + (T(1) - P.g_b) * p.water_drag;
+    F.H_l = Hn[1][0]; F.H_r = Hn[1][2]; F.H_t = Hn[0][1]; F.H_b = Hn[2][1];
+    auto surf = [&](T bed, T H, T& S, T& db) {
+        S = M<T>::max(bed, -rho_ratio<T>() * H) + H;
+        db = T(1) + (bed > -rho_ratio<T>() * H ? T(0) : -rho_ratio<T>());
+    };
+    surf(P.bed_l, F.H_l, F.S_l, F.db_l);
+    surf(P.bed_r, F.H_r, F.S_r, F.db_r);
+    surf(P.bed_t, F.H_t, F.S_t, F.db_t);
+    surf(P.bed_b, F.H_b, F.S_b, F.db_b);
+    F.w_l = (j > 0 && j < nx) ? T(1) : T(0);
+    F.w_r = (j + 1 < nx) ? T(1) : T(0);
+    F.w_t = (i > 0 && i < ny) ? T(1) : T(0);
+    F.w_b = (i + 1 < ny) ? T(1) : T(0);
+    F.bed_c = P.bed_c;
+    F.beta_c = P.beta_c;
+}
+
+// One local Newton step's matrix and residual from the frozen coefficients
+// (same terms and order of rows/columns as assemble<T,true>).
+template <typename T>
+__device__ __forceinline__ void assemble_fast(const Frozen<T>& F, T ul, T ur, T vt, T vb, T Hc, T fu_l, T fu_r,
+                                              T fv_t, T fv_b, T fH, T thk, T dti, const Phys<T>& p, T (&J)[25],
+                                              T (&r)[5]) {
+    const T dxi = p.dxi;
+    const T gc = sigmoid(F.bed_c + rho_ratio<T>() * Hc, p.sig_c);
+    // mass row
+    {
+        Calving<T> cv = calving_g(Hc, gc, p);
+        Flux<T> ql = upwind_flux(ul, F.H_l, Hc, F.w_l > T(0));
+        Flux<T> qr = upwind_flux(ur, Hc, F.H_r, F.w_r > T(0));
+        Flux<T> qt = upwind_flux(vt, Hc, F.H_t, F.w_t > T(0));
+        Flux<T> qb = upwind_flux(vb, F.H_b, Hc, F.w_b > T(0));
+        T r4 = Hc * dti - fH - cv.res - ql.res * dxi + qr.res * dxi + qt.res * dxi - qb.res * dxi;
+        if ((Hc - p.dt * r4) <= thk) {
+            J[20] = T(0); J[21] = T(0); J[22] = T(0); J[23] = T(0); J[24] = T(1);
+            r[4] = Hc - thk;
+        } else {
+            J[20] = -ql.d_vel * dxi;
+            J[21] = qr.d_vel * dxi;
+            J[22] = qt.d_vel * dxi;
+            J[23] = -qb.d_vel * dxi;
+            J[24] = dti - cv.d_H + (-ql.d_Hb + qr.d_Ha + qt.d_Ha - qb.d_Hb) * dxi;
+            r[4] = r4;
+        }
+    }
+    // own-cell normal stresses
+    const T etaH = F.eta_c * Hc;
+    const T pre = T(2) * etaH * dxi;
+    const T exx = T(2) * (ur - ul) * dxi + (vt - vb) * dxi;
+    const T eyy = (ur - ul) * dxi + T(2) * (vt - vb) * dxi;
+    const T sxx = T(2) * etaH * exx, syy = T(2) * etaH * eyy;
+    const T hx = T(2) * exx * F.eta_c * dxi, hy = T(2) * eyy * F.eta_c * dxi;
+    const T p2 = pre * dxi;
+    J[0] = -T(2) * p2; J[1] = T(2) * p2; J[2] = p2; J[3] = -p2; J[4] = hx;
+    J[5] = T(2) * p2; J[6] = -T(2) * p2; J[7] = -p2; J[8] = p2; J[9] = -hx;
+    J[10] = p2; J[11] = -p2; J[12] = -T(2) * p2; J[13] = T(2) * p2; J[14] = -hy;
+    J[15] = -p2; J[16] = p2; J[17] = T(2) * p2; J[18] = -T(2) * p2; J[19] = hy;
+    T r0 = -fu_l + sxx * dxi, r1 = -fu_r - sxx * dxi, r2 = -fv_t - syy * dxi, r3 = -fv_b + syy * dxi;
+    // neighbour normal stresses
+    r0 -= (F.kl * (ul - F.u_ll) + F.cl) * dxi;   J[0] -= F.kl * dxi;
+    r1 += (F.kr * (F.u_rr - ur) + F.cr) * dxi;   J[6] -= F.kr * dxi;
+    r2 += (F.kt * (F.v_tt - vt) + F.ct) * dxi;   J[12] -= F.kt * dxi;
+    r3 -= (F.kb * (vb - F.v_bb) + F.cb) * dxi;   J[18] -= F.kb * dxi;
+    // corner shear stresses
+    {
+        const T ecH = F.ec * Hc;
+        T eH = (F.S_tl + ecH) * F.w_tl;
+        T exy = T(0.5) * ((F.u_tl - ul) * dxi + (vt - F.v_lt) * dxi);
+        T res = T(2) * eH * exy * dxi, dd = eH * dxi * dxi, de = T(2) * exy * F.w_tl * F.ec * dxi;
+        r0 += res; r2 -= res; J[0] -= dd; J[4] += de; J[12] -= dd; J[14] -= de;
+        eH = (F.S_tr + ecH) * F.w_tr;
+        exy = T(0.5) * ((F.u_tr - ur) * dxi + (F.v_rt - vt) * dxi);
+        res = T(2) * eH * exy * dxi; dd = eH * dxi * dxi; de = T(2) * exy * F.w_tr * F.ec * dxi;
+        r1 += res; r2 += res; J[6] -= dd; J[9] += de; J[12] -= dd; J[14] += de;
+        eH = (F.S_bl + ecH) * F.w_bl;
+        exy = T(0.5) * ((ul - F.u_bl) * dxi + (vb - F.v_lb) * dxi);
+        res = T(2) * eH * exy * dxi; dd = eH * dxi * dxi; de = T(2) * exy * F.w_bl * F.ec * dxi;
+        r0 -= res; r3 -= res; J[0] -= dd; J[4] -= de; J[18] -= dd; J[19] -= de;
+        eH = (F.S_br + ecH) * F.w_br;
+        exy = T(0.5) * ((ur - F.u_br) * dxi + (F.v_rb - vb) * dxi);
+        res = T(2) * eH * exy * dxi; dd = eH * dxi * dxi; de = T(2) * exy * F.w_br * F.ec * dxi;
+        r1 -= res; r3 += res; J[6] -= dd; J[9] -= de; J[18] -= dd; J[19] += de;
+    }
+    // basal drag
+    {
+        const T bec = gc * F.beta_c + (T(1) - gc) * p.water_drag;
+        T bl = T(0.5) * (F.be_l + bec), br = T(0.5) * (bec + F.be_r);
+        T bt = T(0.5) * (F.be_t + bec), bb = T(0.5) * (bec + F.be_b);
+        r0 -= bl * ul; r1 -= br * ur; r2 -= bt * vt; r3 -= bb * vb;
+        J[0] -= bl; J[6] -= br; J[12] -= bt; J[18] -= bb;
+        if (p.gl_deriv) {
+            T dgc = rho_ratio<T>() * (p.sig_c * gc * (T(1) - gc)) * (F.beta_c - p.water_drag);
+            J[4] += T(-0.5) * dgc * ul;
+            J[9] += T(-0.5) * dgc * ur;
+            J[14] += T(-0.5) * dgc * vt;
+            J[19] += T(-0.5) * dgc * vb;
+        }
+    }
+    // driving stress; x: left (m) / right (p); y: bottom (m) / top (p)
+    {
+        const T bc = M<T>::max(F.bed_c, -rho_ratio<T>() * Hc);
+        const T Sc = bc + Hc;
+        const T dbc = T(1) + (F.bed_c > -rho_ratio<T>() * Hc ? T(0) : -rho_ratio<T>());
+        // left face: m = left, p = this cell
+        T Havg = T(0.5) * (F.H_l + Hc), dS = Sc - F.S_l;
+        r0 -= Havg * dS * dxi * F.w_l;
+        J[4] -= (T(0.5) * dS * dxi + Havg * dbc * dxi) * F.w_l;
+        // right face: m = this cell, p = right
+        Havg = T(0.5) * (Hc + F.H_r); dS = F.S_r - Sc;
+        r1 -= Havg * dS * dxi * F.w_r;
+        J[9] -= (T(0.5) * dS * dxi - Havg * dbc * dxi) * F.w_r;
+        // top face: m = this cell (bottom), p = top
+        Havg = T(0.5) * (Hc + F.H_t); dS = F.S_t - Sc;
+        r2 -= Havg * dS * dxi * F.w_t;
+        J[14] -= (T(0.5) * dS * dxi - Havg * dbc * dxi) * F.w_t;
+        // bottom face: m = bottom, p = this cell (top)
+        Havg = T(0.5) * (F.H_b + Hc); dS = Sc - F.S_b;
+        r3 -= Havg * dS * dxi * F.w_b;
+        J[19] -= (T(0.5) * dS * dxi + Havg * dbc * dxi) * F.w_b;
+    }
+    r[0] = r0; r[1] = r1; r[2] = r2; r[3] = r3;
+}
+
+// LU solve with the pivot reciprocals reused in the back substitution.
+template <typename T> __device__ __forceinline__ void lu5_solve_fast(T (&A)[25], const T (&b)[5], T (&x)[5]) {
+    T inv[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        inv[k] = T(1) / A[k * 5 + k];
+#pragma unroll
+        for (int i = k + 1; i < 5; i++) {
+            A[i * 5 + k] *= inv[k];
+#pragma unroll
+            for (int j = k + 1; j < 5; j++) A[i * 5 + j] -= A[i * 5 + k] * A[k * 5 + j];
+        }
+    }
+    T y1 = b[1] - A[5] * b[0];
+    T y2 = b[2] - A[10] * b[0] - A[11] * y1;
+    T y3 = b[3] - A[15] * b[0] - A[16] * y1 - A[17] * y2;
+    T y4 = b[4] - A[20] * b[0] - A[21] * y1 - A[22] * y2 - A[23] * y3;
+    x[4] = y4 * inv[4];
+    x[3] = (y3 - A[19] * x[4]) * inv[3];
+    x[2] = (y2 - A[13] * x[3] - A[14] * x[4]) * inv[2];
+    x[1] = (y1 - A[7] * x[2] - A[8] * x[3] - A[9] * x[4]) * inv[1];
+    x[0] = (b[0] - A[1] * x[1] - A[2] * x[2] - A[3] * x[3] - A[4] * x[4]) * inv[0];
+}
+
 // Per-cell Newton deltas.  scratch holds 5 cell arrays: 0.5*du_l, 0.5*du_r,
 // 0.5*dv_t, 0.5*dv_b, dH.
 template <typename T, bool LOCAL>
-__global__ void __launch_bounds__(VNT) vanka_cells_kernel(
+__global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : 1) vanka_cells_kernel(
     T* __restrict__ scratch, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, const T* __restrict__ bed,
     const T* __restrict__ B, const T* __restrict__ beta, const T* __restrict__ gamma, const int* __restrict__ flags,
@@ -238,8 +438,12 @@ __global__ void __launch_bounds__(VNT) vanka_cells_kernel(
     if (i >= ny || j >= nx) return;
     if (LOCAL && !ref_tile_on(flags, i, j, nx)) return;
 
-    Patch<T> P;
-    load_patch(P, s_eta, r, c, u, v, H, bed, beta, i, j, ny, nx, p);
+    Frozen<T> F;
+    {
+        Patch<T> P;
+        load_patch(P, s_eta, r, c, u, v, H, bed, beta, i, j, ny, nx, p);
+        make_frozen(F, P, ny, nx, p);
+    }
     const T ul0 = u[int64_t(i) * (nx + 1) + j], ur0 = u[int64_t(i) * (nx + 1) + j + 1];
     const T vt0 = v[int64_t(i) * nx + j], vb0 = v[int64_t(i + 1) * nx + j];
     const T H0 = H[int64_t(i) * nx + j];
@@ -247,12 +451,13 @@ __global__ void __launch_bounds__(VNT) vanka_cells_kernel(
     const T fv_t = f_v[int64_t(i) * nx + j], fv_b = f_v[int64_t(i + 1) * nx + j];
     const T fH = f_H[int64_t(i) * nx + j];
     const T thk = gamma[int64_t(i) * nx + j];
+    const T dti = T(1) / p.dt;
     T ul = ul0, ur = ur0, vt = vt0, vb = vb0, Hc = H0;
     for (int it = 0; it < n_newton; it++) {
         T J[25], rr[5], x[5];
-        assemble<T, true>(P, ul, ur, vt, vb, Hc, fu_l, fu_r, fv_t, fv_b, fH, thk, ny, nx, p, J, rr);
+        assemble_fast<T>(F, ul, ur, vt, vb, Hc, fu_l, fu_r, fv_t, fv_b, fH, thk, dti, p, J, rr);
         J[0] -= shift; J[6] -= shift; J[12] -= shift; J[18] -= shift; J[24] += shift;  // vanka.cu:406-410
-        lu5_solve(J, rr, x);
+        lu5_solve_fast(J, rr, x);
         ul -= T(0.25) * x[0];
         ur -= T(0.25) * x[1];
         vt -= T(0.25) * x[2];
@@ -423,6 +628,28 @@ int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_
     return (int)cudaGetLastError();
 }
 
+// Only the per-cell Newton kernel, n_launch times (profiling / timing; U is not updated).
+template <typename T>
+int launch_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,
+                       int n_newton, double shift, const int* flags, const int* any_active, void* scratch,
+                       cudaStream_t s) {
+    Geo g{a->ny, a->nx, a->nb};
+    Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
+    for (int k = 0; k < n_launch; k++) {
+        if (flags)
+            vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
+                (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
+                (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags,
+                any_active, n_newton, T(shift), g, p);
+        else
+            vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
+                (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
+                (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr,
+                nullptr, n_newton, T(shift), g, p);
+    }
+    return (int)cudaGetLastError();
+}
+
 template <typename T>
 int launch_error_mask(const GlideLevelArgs* a, const void* r_u, const void* r_v, const void* r_H, double threshold,
                       void* err_mask, int* flags, int* any_active, cudaStream_t s) {
@@ -463,6 +690,8 @@ int launch_vanka_adjoint(const GlideLevelArgs* a, void* l_u, void* l_v, void* l_
 #define INST(T)                                                                                                  \
     template int launch_vanka_sweeps<T>(const GlideLevelArgs*, const void*, const void*, const void*, int, int,   \
                                         double, double, const int*, const int*, void*, cudaStream_t);             \
+    template int launch_vanka_cells<T>(const GlideLevelArgs*, const void*, const void*, const void*, int, int,     \
+                                       double, const int*, const int*, void*, cudaStream_t);                      \
     template int launch_error_mask<T>(const GlideLevelArgs*, const void*, const void*, const void*, double,       \
                                       void*, int*, int*, cudaStream_t);                                           \
     template int launch_tile_flags<T>(const GlideLevelArgs*, const void*, int*, int*, cudaStream_t);              \

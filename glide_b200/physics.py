@@ -18,6 +18,11 @@ Additions (keyword-only):
   forward(guess=(u, v))  start from a supplied velocity guess; the plain
              cycle finishes the solve and the guess is dropped when the first
              cycle fails to cut the residual by ``guess_min_reduction``.
+  forward(tol=..., finish=True)  once a V-cycle cuts |r| by less than
+             ``stall_factor`` (the coarse-grid correction then stops helping:
+             it re-injects an error near 1e-5 relative on these problems),
+             continue with blocks of ``finish_block`` FP64 fine-level Vanka
+             sweeps until the tolerance is met.
   settings   solver settings (``SolverSettings``); defaults = reference.
 """
 from __future__ import annotations
@@ -54,7 +59,8 @@ class IcePhysics:
 
     def __init__(self, ny, nx, dx, n_levels=5, n=3.0, eps_reg=1e-5, thklim=0.1, water_drag=1e-3, calving_rate=1.0,
                  gl_sigmoid_c=0.1, gl_derivatives=False, *, precision="fp32", device=None,
-                 settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0):
+                 settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0,
+                 stall_factor=0.5, finish_block=20, finish_anderson=0, finish_fp32=False):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -70,6 +76,10 @@ class IcePhysics:
         self.batch = int(batch)
         self.use_graphs = bool(use_graphs)
         self.guess_min_reduction = float(guess_min_reduction)
+        self.stall_factor = float(stall_factor)
+        self.finish_block = int(finish_block)
+        self.finish_anderson = int(finish_anderson)
+        self.finish_fp32 = bool(finish_fp32)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
         self.dtype = _PRECISIONS[precision]
@@ -221,11 +231,14 @@ class IcePhysics:
 
     # ------------------------------------------------------------------ API
     def forward(self, dt, n_vcycles=3, verbose=False, update_geometry=True, *, tol=None, max_vcycles=100,
-                guess=None, history=None):
+                guess=None, history=None, finish=True, max_finish_sweeps=4000):
         """One implicit time step (glide/physics.py:141-209).
 
         Without ``tol`` runs ``n_vcycles`` cycles like the reference.  With
-        ``tol`` runs cycles until |r|/|r0| <= tol (or ``max_vcycles``).
+        ``tol`` runs cycles until |r|/|r0| <= tol; with ``finish`` a stalled
+        cycle hands over to FP64 fine-level relaxation (see the module doc).
+        ``last_info`` records cycles, finishing sweeps, the residual reached
+        and whether a guess was used or dropped.
         """
         self._set_dt(dt)
         g = self.grid
@@ -235,7 +248,7 @@ class IcePhysics:
         track = tol is not None or verbose or history is not None or guess is not None
         r0 = self.residual_norm() if track else None
         hist = [1.0] if track else []
-        info = {"vcycles": 0, "guess_used": False, "fallback": False}
+        info = {"vcycles": 0, "finish_sweeps": 0, "guess_used": False, "fallback": False}
         if verbose:
             print(f"  Initial: |r| = {r0:.2e}")
         if guess is not None:
@@ -246,27 +259,37 @@ class IcePhysics:
             info["guess_used"] = True
         n_max = max_vcycles if tol is not None else n_vcycles
         k = 0
+        prev = 1.0
+        rel = 1.0
+        stalled = False
         while k < n_max:
             self._run_cycle()
             k += 1
-            if track:
-                r = self.residual_norm()
-                rel = r / r0 if r0 > 0 else 0.0
-                if guess is not None and k == 1 and info["guess_used"]:
-                    # judge the guess by the first cycle: it must cut |r| by guess_min_reduction
-                    if not (rel * self.guess_min_reduction <= 1.0) or not math.isfinite(rel):
-                        g.U.copy_(saved)
-                        info["fallback"] = True
-                        info["guess_used"] = False
-                        hist.append(float("nan"))
-                        continue
-                hist.append(rel)
-                if verbose:
-                    print(f"  V-cycle {k - 1}: |r|/|r0| = {rel:.2e}")
-                if tol is not None and rel <= tol:
-                    break
+            if not track:
+                continue
+            rel = self.residual_norm() / r0 if r0 > 0 else 0.0
+            if guess is not None and k == 1 and info["guess_used"]:
+                # judge the guess by the first cycle: it must cut |r| by guess_min_reduction
+                if not (rel * self.guess_min_reduction <= 1.0) or not math.isfinite(rel):
+                    g.U.copy_(saved)
+                    info["fallback"] = True
+                    info["guess_used"] = False
+                    hist.append(float("nan"))
+                    rel = 1.0
+                    continue
+            hist.append(rel)
+            if verbose:
+                print(f"  V-cycle {k - 1}: |r|/|r0| = {rel:.2e}")
+            if tol is not None and rel <= tol:
+                break
+            if tol is not None and finish and rel > self.stall_factor * prev:
+                stalled = True
+                break
+            prev = rel
+        if tol is not None and finish and rel > tol and (stalled or k >= n_max):
+            rel = self._finish(r0, tol, max_finish_sweeps, hist, info, verbose)
         info["vcycles"] = k
-        info["rel_residual"] = hist[-1] if hist else None
+        info["rel_residual"] = rel if track else None
         self.last_history = hist
         self.last_info = info
         if history is not None:
@@ -276,6 +299,77 @@ class IcePhysics:
             if self.grid32 is not None:
                 self.grid32.H_prev.copy_(g.H)
         return g.u, g.v, g.H
+
+    def _finish(self, r0, tol, max_sweeps, hist, info, verbose):
+        """Fine-level Vanka relaxation in blocks until |r|/|r0| <= tol.
+
+        Mixed precision with ``finish_fp32``: blocks of FP32 sweeps on the
+        correction problem f32 = F32(fl32(U64)) - r64 while they still cut the
+        FP64 residual, then FP64 sweeps.  ``finish_anderson`` = m > 0 applies
+        Anderson acceleration (depth m) over the blocks to the velocity part.
+        """
+        g = self.grid
+        st = self.settings
+        g.gamma.fill_(self.thklim)
+        rel = hist[-1] if hist else 1.0
+        done = 0
+        use32 = self.grid32 is not None and self.finish_fp32
+        m = self.finish_anderson
+        nU = g.nb * (g.nu + g.nv)
+        Fs, Gs = [], []
+        prev = rel
+        while done < max_sweeps and rel > tol:
+            x0 = g.U[:nU].clone() if m > 0 else None
+            if use32:
+                self._fp32_sweeps(self.finish_block)
+            else:
+                g.vanka_sweep(self.finish_block, n_inner=st.n_newton, omega=st.omega, shift=st.shift)
+            done += self.finish_block
+            if m > 0:
+                Gx = g.U[:nU].clone()
+                f = Gx - x0
+                Fs.append(f)
+                Gs.append(Gx)
+                if len(Fs) > m + 1:
+                    Fs.pop(0)
+                    Gs.pop(0)
+                if len(Fs) > 1:
+                    dF = torch.stack([Fs[k + 1] - Fs[k] for k in range(len(Fs) - 1)], 1)
+                    dG = torch.stack([Gs[k + 1] - Gs[k] for k in range(len(Gs) - 1)], 1)
+                    gam = torch.linalg.lstsq(dF, f.unsqueeze(1)).solution.squeeze(1)
+                    g.U[:nU] = Gx - dG @ gam
+            rel = self.residual_norm() / r0 if r0 > 0 else 0.0
+            hist.append(rel)
+            if verbose:
+                print(f"  finish {done} sweeps ({'fp32' if use32 else 'fp64'}): |r|/|r0| = {rel:.2e}")
+            if not math.isfinite(rel):
+                break
+            if use32 and rel > 0.7 * prev:
+                use32 = False           # FP32 correction floor reached: continue in FP64
+                Fs, Gs = [], []
+            prev = rel
+        info["finish_sweeps"] = done
+        return rel
+
+    def _fp32_sweeps(self, n):
+        """FP32 fine-level sweeps on the FP64 problem's correction equation."""
+        g64, g32 = self.grid, self.grid32
+        lib = self.kernels
+        s = N.stream_handle()
+        st = self.settings
+        ntot = g64.nb * g64.n_total
+        g64.compute_residual()
+        N.check(lib.glide_convert(N.F32, g32.U.data_ptr(), g64.U.data_ptr(), ntot, 0, s), "convert")
+        N.check(lib.glide_convert(N.F32, g32.r.data_ptr(), g64.r.data_ptr(), ntot, 0, s), "convert")
+        g32.w.copy_(g32.U)
+        g32.gamma.fill_(self.thklim)
+        a = g32.level_args()
+        N.check(lib.glide_residual(C.byref(a), g32.r_u.data_ptr(), g32.r_v.data_ptr(), g32.r_H.data_ptr(),
+                                   g32.f_u.data_ptr(), g32.f_v.data_ptr(), g32.f_H.data_ptr(), s), "residual32")
+        g32.vanka_sweep(n, n_inner=st.n_newton, omega=st.omega, shift=st.shift)
+        N.check(lib.glide_lincomb(N.F32, g32.z.data_ptr(), g32.U.data_ptr(), 1.0, g32.w.data_ptr(), -1.0, ntot, s),
+                "lincomb")
+        N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.z.data_ptr(), ntot, 1, s), "convert")
 
     def adjoint(self, dL_du, dL_dv, dL_dH, n_vcycles=2, *, tol=None, max_vcycles=100, exact=False):
         """grad_beta of a loss through one implicit step (glide/physics.py:211-242).

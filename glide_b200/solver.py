@@ -31,6 +31,7 @@ class SolverSettings:
     adj_smooth: int = 10
     adj_omega: float = 1.0
     exact_adjoint: bool = False  # reference VJP/grad boundary handling when False
+    smooth_H_correction: bool = False  # bilinear instead of injected coarse H correction
 
     def native(self, thklim) -> N.SolverConfig:
         c = N.SolverConfig()
@@ -40,6 +41,7 @@ class SolverSettings:
         c.omega, c.shift, c.err_threshold = float(self.omega), float(self.shift), float(self.err_threshold)
         c.adj_coarse, c.adj_smooth, c.adj_omega = self.adj_coarse, self.adj_smooth, float(self.adj_omega)
         c.exact_adjoint = int(self.exact_adjoint)
+        c.smooth_H_correction = int(self.smooth_H_correction)
         return c
 
 

@@ -84,6 +84,11 @@ int glide_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, v
 int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                        int n_newton, double omega, double shift, const int* flags, const int* any_active,
                        void* scratch, void* stream);
+/* Only the per-cell local Newton kernel of a sweep, n_launch times, writing the
+ * per-cell deltas into scratch without updating U (profiling and timing). */
+int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,
+                      int n_newton, double shift, const int* flags, const int* any_active, void* scratch,
+                      void* stream);
 /* err_mask = (|r_u|+|r_u|+|r_v|+|r_v|+|FB(r_H,H-gamma)| > threshold); if flags
  * is non-null also the per-reference-block flags ((ny/14+1)*(nx/14+1)*nb ints)
  * and any_active (nb ints). */
@@ -134,6 +139,7 @@ typedef struct GlideSolverConfig {
     int adj_coarse, adj_smooth;
     double adj_omega;
     int exact_adjoint;      /* 0: reference VJP boundary handling */
+    int smooth_H_correction;/* 0: inject the coarse H correction (reference), 1: bilinear */
 } GlideSolverConfig;
 
 /* One FASCD V-cycle from level k0 (finest=1 sets w=U, chi=gamma-H first). */

@@ -245,7 +245,7 @@ def _assemble(fz: _Frozen, ul, ur, vt, vb, Hc, p: Params, dx, dt, with_res, f=No
 
 
 def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt, n_newton=10, cell_on=None,
-                 shift=1.0):
+                 shift=1.0, return_cells=False):
     """Delta arrays written by one ``vanka_smooth`` launch (vanka.cu:3-439).
 
     Each cell runs ``n_newton`` damped (0.25) Newton steps on its 5 unknowns
@@ -277,6 +277,8 @@ def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt,
     d_ur = np.where(on, 0.5 * (ur - ur0), 0.0)
     d_vt = np.where(on, 0.5 * (vt - vt0), 0.0)
     d_vb = np.where(on, 0.5 * (vb - vb0), 0.0)
+    if return_cells:
+        return d_ul, d_ur, d_vt, d_vb, np.where(on, Hc - Hc0, 0.0)
     du = np.zeros((ny, nx + 1)); dv = np.zeros((ny + 1, nx))
     du[:, :nx] += d_ul
     du[:, 1:] += d_ur

@@ -5,10 +5,13 @@ kernels (compiled from the reference tree, ``--use_fast_math``) on seeded
 inputs, written by ``tests/golden/make_golden.py`` on a GPU box.  The oracle,
 run in FP64 on the same (FP32-rounded) inputs, must agree within FP32
 tolerances, stated per case below as norm-wise relative error:
-  single operators (residual, JVP, VJP, grad, transfers)   <= 2e-5
-  one Vanka sweep / local sweep / adjoint sweep pair       <= 1e-4
-  one forward step (1 V-cycle, 3 levels, 200 coarse sweeps) <= 5e-3
-  one adjoint V-cycle gradient                             <= 5e-3
+  single operators (residual, JVP, VJP, grad)               <= 2e-6
+  transfers                                                 <= 2e-7
+  one Vanka sweep / local sweep / adjoint sweep pair        <= 1e-4
+  one forward step (1 V-cycle, 3 levels, 200 coarse sweeps) <= 2e-5
+  one adjoint V-cycle gradient                              <= 2e-5
+(measured when the fixture was made: residual 4.5e-7, JVP/VJP <= 2.8e-7,
+forward step 2.1e-6, adjoint gradient 2.1e-6)
 """
 import os
 
@@ -43,7 +46,7 @@ def test_residual(gold):
                                                           "beta", "mask", "gamma")
     r = ssa.residual(u, v, H, fu, fv, fH, bed, B, beta, mask, gamma, Params(), gold["dx"], gold["dt"])
     for a, k in zip(r, ("out_r_u", "out_r_v", "out_r_H")):
-        assert rel(a, gold[k]) <= 2e-5
+        assert rel(a, gold[k]) <= 2e-6
 
 
 @pytest.mark.parametrize("gl", [0, 1])
@@ -53,17 +56,17 @@ def test_jvp_vjp(gold, gl):
     p = Params(gl_derivatives=bool(gl))
     j = ssa.jvp(u, v, H, du, dv, dH, bed, B, beta, mask, gamma, p, gold["dx"], gold["dt"])
     for a, k in zip(j, "uvH"):
-        assert rel(a, gold[f"out_jvp{gl}_{k}"]) <= 2e-5
+        assert rel(a, gold[f"out_jvp{gl}_{k}"]) <= 2e-6
     fu, fv, fH = _in(gold, "f_u", "f_v", "f_H")
     l = ssa.vjp(u, v, H, fu, fv, fH, bed, B, beta, mask, gamma, p, gold["dx"], gold["dt"])
     for a, k in zip(l, "uvH"):
-        assert rel(a, gold[f"out_vjp{gl}_{k}"]) <= 2e-5
+        assert rel(a, gold[f"out_vjp{gl}_{k}"]) <= 2e-6
 
 
 def test_grad_beta(gold):
     u, v, H, du, dv, bed, beta = _in(gold, "u", "v", "H", "d_u", "d_v", "bed", "beta")
     g = ssa.grad_beta(u, v, H, du, dv, bed, beta, Params(), exact_boundary=False)
-    assert rel(g, gold["out_grad_beta"]) <= 2e-5
+    assert rel(g, gold["out_grad_beta"]) <= 2e-6
 
 
 @pytest.mark.parametrize("local", [False, True])
@@ -115,8 +118,8 @@ def test_forward_and_adjoint_step(gold):
     ph.set_geometry(f32(c.bed), f32(c.thickness))
     ph.set_parameters(B=f32(c.B), beta=f32(c.beta), smb=f32(c.smb))
     u, v, H = ph.forward(c.dt, n_vcycles=1)
-    assert rel(u, gold["step_u"]) <= 5e-3
-    assert rel(v, gold["step_v"]) <= 5e-3
-    assert rel(H, gold["step_H"]) <= 5e-3
+    assert rel(u, gold["step_u"]) <= 2e-5
+    assert rel(v, gold["step_v"]) <= 2e-5
+    assert rel(H, gold["step_H"]) <= 2e-5
     g = ph.adjoint(gold["step_dLu"], gold["step_dLv"], np.zeros((32, 32)), n_vcycles=1)
-    assert rel(g, gold["step_grad_beta"]) <= 5e-3
+    assert rel(g, gold["step_grad_beta"]) <= 2e-5
