@@ -193,6 +193,11 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
+def launches(runner):
+    from glide_b200 import _native as N
+    return N.load().glide_launch_count() + runner.ph.graph_launches
+
+
 def time_steps(runner, devs, warmup, steps, world, flush):
     import torch
     infos = []
@@ -200,15 +205,18 @@ def time_steps(runner, devs, warmup, steps, world, flush):
         runner.step(devs[k % len(devs)])
     torch.cuda.synchronize()
     total = 0.0
+    runner.launches = 0
     for k in range(steps):
         flush_l2(flush)
         barrier(world)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = launches(runner)
         a.record()
         infos.append(runner.step(devs[warmup + k]))
         b.record()
         torch.cuda.synchronize()
+        runner.launches += launches(runner) - l0
         total += a.elapsed_time(b) / 1e3
     return total, infos
 
@@ -361,7 +369,7 @@ def run_ours(args):
                                "vcycles_per_step": [i.get("vcycles") for i in info_plain],
                                "rel_residual_reached": [i.get("rel_residual") for i in info_plain]},
             "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": None,
+            "gpu_launches": fast.launches,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),

@@ -22,7 +22,7 @@ SYMBOLS = [
     "glide_tile_flags", "glide_vanka_adjoint", "glide_restrict", "glide_prolong", "glide_lincomb", "glide_fill",
     "glide_mask_le", "glide_convert", "glide_norms", "glide_norm_parts", "glide_fascd_vcycle",
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
-    "glide_graph_destroy", "glide_version",
+    "glide_graph_destroy", "glide_launch_count", "glide_version",
 ]
 
 
@@ -98,12 +98,13 @@ def load():
         "glide_graph_create": [C.POINTER(Level), i, C.POINTER(SolverConfig), i, C.POINTER(C.c_void_p)],
         "glide_graph_launch": [vp, vp],
         "glide_graph_destroy": [vp],
+        "glide_launch_count": [],
         "glide_version": [],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
-        f.restype = C.c_char_p if name == "glide_version" else C.c_int
+        f.restype = C.c_char_p if name == "glide_version" else (C.c_longlong if name == "glide_launch_count" else C.c_int)
     _lib = lib
     return lib
 

@@ -4,6 +4,7 @@
 // glide/solver.py:71-220 as device-side launches on one stream (no host
 // synchronisation inside a cycle), so a whole cycle can be captured once into
 // a CUDA graph and replayed (glide_graph_*).
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -11,6 +12,10 @@
 #include "glide_common.cuh"
 
 namespace glide {
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_total() { return g_launches.load(std::memory_order_relaxed); }
+
 template <typename T> int launch_residual(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*, cudaStream_t);
 template <typename T> int launch_jvp(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*, cudaStream_t);
 template <typename T> int launch_vjp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*, void*, void*, void*, int, cudaStream_t);
@@ -56,6 +61,8 @@ static int check_level(const GlideLevelArgs* a) {
 extern "C" {
 
 const char* glide_version(void) { return "glide_b200 0.1 (sm_100a)"; }
+
+long long glide_launch_count(void) { return glide::launch_total(); }
 
 int glide_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, void* r_u, void* r_v,
                    void* r_H, void* stream) {
@@ -197,6 +204,7 @@ int glide_convert(int dst_dtype, void* out, const void* x, int64_t n, int accumu
     if (!out || !x) return GLIDE_E_NULL;
     if (n <= 0) return GLIDE_OK;
     unsigned nb = unsigned((n + 255) / 256);
+    glide::count_launch();
     if (dst_dtype == GLIDE_F32) convert_k<float, double><<<nb, 256, 0, S(stream)>>>((float*)out, (const double*)x, n, accumulate);
     else convert_k<double, float><<<nb, 256, 0, S(stream)>>>((double*)out, (const float*)x, n, accumulate);
     return (int)cudaGetLastError();

@@ -14,6 +14,11 @@
 
 namespace glide {
 
+// host-side count of kernel launches issued by this library (also counts
+// launches recorded during stream capture); see glide_launch_count
+void count_launch();
+long long launch_total();
+
 // --------------------------------------------------------------------------
 // precision helpers
 // --------------------------------------------------------------------------

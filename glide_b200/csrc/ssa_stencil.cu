@@ -485,7 +485,7 @@ int launch_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, c
                     void* r_H, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    stencil_kernel<T, false><<<tile_grid(g), NTHR, 0, s>>>(
+    glide::count_launch(), stencil_kernel<T, false><<<tile_grid(g), NTHR, 0, s>>>(
         (T*)r_u, (T*)r_v, (T*)r_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
         (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
         (const T*)a->gamma, g, p);
@@ -497,7 +497,7 @@ int launch_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const 
                void* j_H, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    stencil_kernel<T, true><<<tile_grid(g), NTHR, 0, s>>>(
+    glide::count_launch(), stencil_kernel<T, true><<<tile_grid(g), NTHR, 0, s>>>(
         (T*)j_u, (T*)j_v, (T*)j_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)d_u, (const T*)d_v,
         (const T*)d_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
         (const T*)a->gamma, g, p);
@@ -511,7 +511,7 @@ int launch_vjp(const GlideLevelArgs* a, const void* l_u, const void* l_v, const 
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     int rf = f_u != nullptr;
-    vjp_kernel<T><<<tile_grid(g, VTY), NTHR, 0, s>>>(
+    glide::count_launch(), vjp_kernel<T><<<tile_grid(g, VTY), NTHR, 0, s>>>(
         (T*)o_u, (T*)o_v, (T*)o_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)l_u, (const T*)l_v,
         (const T*)l_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask, (const T*)f_u,
         (const T*)f_v, (const T*)f_H, rf, exact_boundary, g, p);
@@ -525,7 +525,7 @@ int launch_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, 
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     dim3 blk(32, 8);
     dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, g.nb);
-    grad_beta_kernel<T><<<grd, blk, 0, s>>>((T*)grad, (const T*)a->u, (const T*)a->v, (const T*)a->H,
+    glide::count_launch(), grad_beta_kernel<T><<<grd, blk, 0, s>>>((T*)grad, (const T*)a->u, (const T*)a->v, (const T*)a->H,
                                             (const T*)l_u, (const T*)l_v, (const T*)a->bed, (const T*)a->beta,
                                             exact_boundary, g, p);
     return (int)cudaGetLastError();

@@ -1,0 +1,218 @@
+// BF16 tensor-core GEMM on the 5th-generation tensor cores (tcgen05 + TMEM)
+// for the learned initial guess (3x3 convolutions as im2col GEMMs).
+//
+//   C[M,N] (+)= A[M,K] * B[N,K]^T   (A, B: BF16, K-major; accumulate FP32 in TMEM)
+//   epilogue: + bias[N], ReLU, store FP32 or BF16, or add into FP32 C.
+//
+// One CTA (4 warps) owns a 128 x 64 tile of C.  Per 64-wide K chunk every
+// thread stages 16-byte rows of A and B into shared memory in the UMMA
+// canonical K-major no-swizzle layout (8-row x 16-byte core matrices,
+// LBO = 128 B between the K halves, SBO = 1024 B between 8-row groups);
+// one elected thread issues four tcgen05.mma (M=128, N=64, K=16) into a
+// 64-column TMEM accumulator and commits them to an mbarrier, which all
+// threads wait on before the next chunk overwrites the tile.  The epilogue
+// reads TMEM with tcgen05.ld (each warp its 32-lane subpartition).
+//
+// Every wait is bounded: after ~1 s the kernel sets *err = 1, stops issuing,
+// waits (bounded) for its own MMAs, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "glide_b200.h"
+
+namespace glide {
+void count_launch();
+}
+
+namespace glide {
+
+constexpr int GM = 128, GN = 64, GK = 64, GTHREADS = 128;
+constexpr uint32_t TMEM_COLS = 64;
+constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory matrix descriptor, K-major, no swizzle (SM100 version 1).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFFu);
+    d |= uint64_t((lbo_bytes >> 4) & 0x3FFFu) << 16;
+    d |= uint64_t((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= uint64_t(1) << 46;
+    return d;
+}
+
+// Instruction descriptor: D = F32, A = B = BF16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try(addr, parity)) {
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    }
+    return true;
+}
+
+// offset of element (row, k) inside a [rows x GK] canonical tile
+__device__ __forceinline__ uint32_t tile_off(int row, int kc) {
+    return uint32_t((row >> 3) * 1024 + kc * 128 + (row & 7) * 16);
+}
+
+// Stage rows [r0, r0+R) x cols [k0, k0+GK) of a K-major BF16 matrix (ld elements).
+template <int R>
+__device__ __forceinline__ void stage_tile(uint8_t* s, const __nv_bfloat16* __restrict__ g, int rows, int K, int ld,
+                                           int r0, int k0) {
+    for (int idx = threadIdx.x; idx < R * (GK / 8); idx += GTHREADS) {
+        const int row = idx / (GK / 8), kc = idx % (GK / 8);
+        const int gr = r0 + row, gk = k0 + kc * 8;
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (gr < rows && gk < K) {
+            const __nv_bfloat16* src = g + int64_t(gr) * ld + gk;
+            if (gk + 8 <= K && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+                val = *reinterpret_cast<const uint4*>(src);
+            } else {
+                __nv_bfloat16 tmp[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) tmp[e] = (gk + e < K) ? src[e] : __float2bfloat16(0.0f);
+                val = *reinterpret_cast<uint4*>(tmp);
+            }
+        }
+        *reinterpret_cast<uint4*>(s + tile_off(row, kc)) = val;
+    }
+}
+
+// out_mode: 0 = store FP32, 1 = store BF16, 2 = add into FP32
+__global__ void __launch_bounds__(GTHREADS) tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, int lda,
+                                                           const __nv_bfloat16* __restrict__ B, int ldb, void* C,
+                                                           int ldc, int M, int N, int K,
+                                                           const float* __restrict__ bias, int relu, int out_mode,
+                                                           int* err) {
+    __shared__ __align__(1024) uint8_t sA[GM * GK * 2];
+    __shared__ __align__(1024) uint8_t sB[GN * GK * 2];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN;
+    const uint32_t mbar_addr = smem_u32(&mbar);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_addr));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    const uint32_t idesc = idesc_bf16_f32(GM, GN);
+    const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+    uint32_t phase = 0;
+    bool ok = true;
+    const int nchunks = (K + GK - 1) / GK;
+    for (int ch = 0; ch < nchunks && ok; ch++) {
+        const int k0 = ch * GK;
+        stage_tile<GM>(sA, A, M, K, lda, m0, k0);
+        stage_tile<GN>(sB, B, N, K, ldb, n0, k0);
+        // make the generic-proxy smem writes visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int s = 0; s < GK / 16; s++) {
+                const uint64_t da = umma_desc(a_base + s * 256, 128, 1024);
+                const uint64_t db = umma_desc(b_base + s * 256, 128, 1024);
+                const uint32_t acc = (ch > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             mbar_addr)
+                         : "memory");
+        }
+        // every thread waits for the MMAs that read the staged tile; the
+        // outcome is made uniform so all threads leave the loop together
+        const int mine = mbar_wait_bounded(mbar_addr, phase) ? 1 : 0;
+        ok = __syncthreads_and(mine) != 0;
+        if (!ok) break;
+        phase ^= 1u;
+    }
+    if (!ok) {
+        if (threadIdx.x == 0 && err) atomicExch(err, 1);
+        mbar_wait_bounded(mbar_addr, phase);   // bounded drain of the MMAs still in flight
+        __syncthreads();
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (ok && nchunks > 0) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < GN; c0 += 8) {
+            uint32_t r[8];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                : "r"(taddr + uint32_t(c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int col = n0 + c0 + e;
+                    if (col >= N) continue;
+                    float x = __uint_as_float(r[e]);
+                    if (bias) x += bias[col];
+                    if (relu) x = fmaxf(x, 0.0f);
+                    const int64_t o = int64_t(row) * ldc + col;
+                    if (out_mode == 0) reinterpret_cast<float*>(C)[o] = x;
+                    else if (out_mode == 1) reinterpret_cast<__nv_bfloat16*>(C)[o] = __float2bfloat16(x);
+                    else reinterpret_cast<float*>(C)[o] += x;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+}  // namespace glide
+
+extern "C" int glide_gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
+                               const float* bias, int relu, int out_mode, int* err, void* stream) {
+    if (!A || !B || !C) return GLIDE_E_NULL;
+    if (M < 1 || N < 1 || K < 1 || lda < K || ldb < K || ldc < N || out_mode < 0 || out_mode > 2) return GLIDE_E_SHAPE;
+    dim3 grid((M + glide::GM - 1) / glide::GM, (N + glide::GN - 1) / glide::GN);
+    glide::count_launch(), glide::tc_gemm_kernel<<<grid, glide::GTHREADS, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err);
+    return (int)cudaGetLastError();
+}

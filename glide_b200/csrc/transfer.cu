@@ -211,16 +211,16 @@ int launch_restrict(int field, int use_max, const void* fine, void* coarse, int 
                     cudaStream_t s) {
     const int nyf = 2 * nyc, nxf = 2 * nxc;
     if (field == 0) {
-        restrict_u_k<T><<<dim3(nblk(int64_t(nyc) * (nxc + 1)), nb), EW, 0, s>>>(
+        glide::count_launch(), restrict_u_k<T><<<dim3(nblk(int64_t(nyc) * (nxc + 1)), nb), EW, 0, s>>>(
             (const T*)fine, (T*)coarse, nyc, nxc, int64_t(nyf) * (nxf + 1), int64_t(nyc) * (nxc + 1));
     } else if (field == 1) {
-        restrict_v_k<T><<<dim3(nblk(int64_t(nyc + 1) * nxc), nb), EW, 0, s>>>(
+        glide::count_launch(), restrict_v_k<T><<<dim3(nblk(int64_t(nyc + 1) * nxc), nb), EW, 0, s>>>(
             (const T*)fine, (T*)coarse, nyc, nxc, int64_t(nyf + 1) * nxf, int64_t(nyc + 1) * nxc);
     } else if (use_max) {
-        restrict_c_k<T, true><<<dim3(nblk(int64_t(nyc) * nxc), nb), EW, 0, s>>>(
+        glide::count_launch(), restrict_c_k<T, true><<<dim3(nblk(int64_t(nyc) * nxc), nb), EW, 0, s>>>(
             (const T*)fine, (T*)coarse, nyc, nxc, int64_t(nyf) * nxf, int64_t(nyc) * nxc);
     } else {
-        restrict_c_k<T, false><<<dim3(nblk(int64_t(nyc) * nxc), nb), EW, 0, s>>>(
+        glide::count_launch(), restrict_c_k<T, false><<<dim3(nblk(int64_t(nyc) * nxc), nb), EW, 0, s>>>(
             (const T*)fine, (T*)coarse, nyc, nxc, int64_t(nyf) * nxf, int64_t(nyc) * nxc);
     }
     return (int)cudaGetLastError();
@@ -232,31 +232,31 @@ int launch_prolong(int field, int smooth, int add, const void* coarse, void* fin
     const int nyf = 2 * nyc, nxf = 2 * nxc;
     int64_t nf = field == 0 ? int64_t(nyf) * (nxf + 1) : field == 1 ? int64_t(nyf + 1) * nxf : int64_t(nyf) * nxf;
     int64_t ncs = field == 0 ? int64_t(nyc) * (nxc + 1) : field == 1 ? int64_t(nyc + 1) * nxc : int64_t(nyc) * nxc;
-    prolong_k<T><<<dim3(nblk(nf), nb), EW, 0, s>>>(field, smooth, add, (const T*)coarse, (T*)fine, nyc, nxc, ncs, nf);
+    glide::count_launch(), prolong_k<T><<<dim3(nblk(nf), nb), EW, 0, s>>>(field, smooth, add, (const T*)coarse, (T*)fine, nyc, nxc, ncs, nf);
     return (int)cudaGetLastError();
 }
 
 template <typename T>
 int launch_lincomb(void* out, const void* x, double a, const void* y, double b, int64_t n, cudaStream_t s) {
     if (n <= 0) return 0;
-    lincomb_k<T><<<nblk(n), EW, 0, s>>>((T*)out, (const T*)x, T(a), (const T*)y, T(b), n);
+    glide::count_launch(), lincomb_k<T><<<nblk(n), EW, 0, s>>>((T*)out, (const T*)x, T(a), (const T*)y, T(b), n);
     return (int)cudaGetLastError();
 }
 template <typename T> int launch_fill(void* out, double val, int64_t n, cudaStream_t s) {
     if (n <= 0) return 0;
-    fill_k<T><<<nblk(n), EW, 0, s>>>((T*)out, T(val), n);
+    glide::count_launch(), fill_k<T><<<nblk(n), EW, 0, s>>>((T*)out, T(val), n);
     return (int)cudaGetLastError();
 }
 template <typename T>
 int launch_mask_le(void* mask, const void* H, const void* gamma, double tol, int64_t n, cudaStream_t s) {
     if (n <= 0) return 0;
-    mask_le_k<T><<<nblk(n), EW, 0, s>>>((T*)mask, (const T*)H, (const T*)gamma, T(tol), n);
+    glide::count_launch(), mask_le_k<T><<<nblk(n), EW, 0, s>>>((T*)mask, (const T*)H, (const T*)gamma, T(tol), n);
     return (int)cudaGetLastError();
 }
 template <typename T>
 int launch_constraint_down(void* chi_c, void* gamma_f, const void* chi_f, const void* wH_f, int nyc, int nxc, int nb,
                            cudaStream_t s) {
-    constraint_down_k<T><<<dim3(nblk(int64_t(nyc) * nxc), nb), EW, 0, s>>>(
+    glide::count_launch(), constraint_down_k<T><<<dim3(nblk(int64_t(nyc) * nxc), nb), EW, 0, s>>>(
         (T*)chi_c, (T*)gamma_f, (const T*)chi_f, (const T*)wH_f, nyc, nxc, int64_t(4) * nyc * nxc,
         int64_t(nyc) * nxc);
     return (int)cudaGetLastError();
@@ -273,9 +273,9 @@ template <typename T>
 int launch_norms(double* out3, double* parts, const void* r_u, const void* r_v, const void* r_H, const void* H,
                  const void* gamma, int64_t nu, int64_t nv, int64_t nc, cudaStream_t s) {
     const int nb = norms_parts_count(nu > nc ? nu : nc);
-    norms_partial_k<T><<<nb, RB, 0, s>>>(parts, (const T*)r_u, (const T*)r_v, (const T*)r_H, (const T*)H,
+    glide::count_launch(), norms_partial_k<T><<<nb, RB, 0, s>>>(parts, (const T*)r_u, (const T*)r_v, (const T*)r_H, (const T*)H,
                                          (const T*)gamma, nu, nv, nc);
-    norms_final_k<<<1, 32, 0, s>>>(out3, parts, nb);
+    glide::count_launch(), norms_final_k<<<1, 32, 0, s>>>(out3, parts, nb);
     return (int)cudaGetLastError();
 }
 

@@ -612,16 +612,16 @@ int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_
     T* H = (T*)a->H;
     for (int k = 0; k < n_iter; k++) {
         if (flags) {
-            vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
+            glide::count_launch(), vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, u, v, H, (const T*)f_u, (const T*)f_v, (const T*)f_H, (const T*)a->bed,
                 (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags, any_active, n_newton, T(shift), g, p);
-            vanka_apply_kernel<T, true><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, flags,
+            glide::count_launch(), vanka_apply_kernel<T, true><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, flags,
                                                                                any_active, T(omega), g);
         } else {
-            vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
+            glide::count_launch(), vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, u, v, H, (const T*)f_u, (const T*)f_v, (const T*)f_H, (const T*)a->bed,
                 (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr, nullptr, n_newton, T(shift), g, p);
-            vanka_apply_kernel<T, false><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, nullptr,
+            glide::count_launch(), vanka_apply_kernel<T, false><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, nullptr,
                                                                                 nullptr, T(omega), g);
         }
     }
@@ -637,12 +637,12 @@ int launch_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     for (int k = 0; k < n_launch; k++) {
         if (flags)
-            vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
+            glide::count_launch(), vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
                 (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags,
                 any_active, n_newton, T(shift), g, p);
         else
-            vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
+            glide::count_launch(), vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
                 (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr,
                 nullptr, n_newton, T(shift), g, p);
@@ -656,12 +656,12 @@ int launch_error_mask(const GlideLevelArgs* a, const void* r_u, const void* r_v,
     Geo g{a->ny, a->nx, a->nb};
     dim3 blk(32, 8);
     dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, g.nb);
-    error_mask_kernel<T><<<grd, blk, 0, s>>>((T*)err_mask, (const T*)r_u, (const T*)r_v, (const T*)r_H,
+    glide::count_launch(), error_mask_kernel<T><<<grd, blk, 0, s>>>((T*)err_mask, (const T*)r_u, (const T*)r_v, (const T*)r_H,
                                              (const T*)a->H, (const T*)a->gamma, T(threshold), g);
     if (flags) {
         cudaMemsetAsync(any_active, 0, sizeof(int) * g.nb, s);
         dim3 tg(g.nx / REF_STRIDE + 1, g.ny / REF_STRIDE + 1, g.nb);
-        tile_flags_kernel<T><<<tg, dim3(REF_WIN, REF_WIN), 0, s>>>(flags, any_active, (const T*)err_mask, g);
+        glide::count_launch(), tile_flags_kernel<T><<<tg, dim3(REF_WIN, REF_WIN), 0, s>>>(flags, any_active, (const T*)err_mask, g);
     }
     return (int)cudaGetLastError();
 }
@@ -671,7 +671,7 @@ int launch_tile_flags(const GlideLevelArgs* a, const void* err_mask, int* flags,
     Geo g{a->ny, a->nx, a->nb};
     cudaMemsetAsync(any_active, 0, sizeof(int) * g.nb, s);
     dim3 tg(g.nx / REF_STRIDE + 1, g.ny / REF_STRIDE + 1, g.nb);
-    tile_flags_kernel<T><<<tg, dim3(REF_WIN, REF_WIN), 0, s>>>(flags, any_active, (const T*)err_mask, g);
+    glide::count_launch(), tile_flags_kernel<T><<<tg, dim3(REF_WIN, REF_WIN), 0, s>>>(flags, any_active, (const T*)err_mask, g);
     return (int)cudaGetLastError();
 }
 
@@ -680,7 +680,7 @@ int launch_vanka_adjoint(const GlideLevelArgs* a, void* l_u, void* l_v, void* l_
                          const void* ra_H, int color, double omega, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    vanka_adjoint_kernel<T><<<cell_grid(g), VNT, 0, s>>>(
+    glide::count_launch(), vanka_adjoint_kernel<T><<<cell_grid(g), VNT, 0, s>>>(
         (T*)l_u, (T*)l_v, (T*)l_H, (const T*)ra_u, (const T*)ra_v, (const T*)ra_H, (const T*)a->u, (const T*)a->v,
         (const T*)a->H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask, color, T(omega), g,
         p);

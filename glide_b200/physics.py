@@ -85,6 +85,7 @@ class IcePhysics:
         self.dtype = _PRECISIONS[precision]
         self._init_hierarchy()
         self._graphs = {}
+        self.graph_launches = 0
         self.last_history = []
         self.last_info = {}
 
@@ -205,22 +206,28 @@ class IcePhysics:
             self._vcycle_native()
 
     def _run_cycle(self):
-        """One V-cycle (or defect-correction step), replayed from a CUDA graph."""
+        """One V-cycle (or defect-correction step), replayed from a CUDA graph.
+
+        ``graph_launches`` accumulates the kernel launches executed by graph
+        replays (the library's own counter sees a captured launch once, at
+        capture)."""
         if not self.use_graphs:
             self._cycle()
             return
         key = (float(self.grid.dt),)
-        gr = self._graphs.get(key)
-        if gr is None:
-            # capture on a side stream; the kernels allocate nothing
-            self._cycle()  # warm-up launch (also checks arguments)
+        entry = self._graphs.get(key)
+        if entry is None:
+            self._cycle()  # warm-up launch (also checks arguments); does this cycle's work
             torch.cuda.synchronize()
             gr = torch.cuda.CUDAGraph()
+            c0 = self.kernels.glide_launch_count()
             with torch.cuda.graph(gr):
                 self._cycle()  # recorded, not executed
-            self._graphs[key] = gr
-            return  # the warm-up call already did this cycle's work
+            self._graphs[key] = (gr, self.kernels.glide_launch_count() - c0)
+            return
+        gr, nodes = entry
         gr.replay()
+        self.graph_launches += nodes
 
     def residual_norm(self):
         """|r| of the finest level with gamma = thklim (glide/physics.py:176-186); FP64, host float."""
@@ -336,7 +343,10 @@ class IcePhysics:
                 if len(Fs) > 1:
                     dF = torch.stack([Fs[k + 1] - Fs[k] for k in range(len(Fs) - 1)], 1)
                     dG = torch.stack([Gs[k + 1] - Gs[k] for k in range(len(Gs) - 1)], 1)
-                    gam = torch.linalg.lstsq(dF, f.unsqueeze(1)).solution.squeeze(1)
+                    # least squares min |f - dF gam| via the (tiny) normal equations
+                    Gm = dF.T @ dF
+                    Gm = Gm + 1e-12 * torch.trace(Gm) * torch.eye(Gm.shape[0], dtype=Gm.dtype, device=Gm.device)
+                    gam = torch.linalg.solve(Gm, dF.T @ f)
                     g.U[:nU] = Gx - dG @ gam
             rel = self.residual_norm() / r0 if r0 > 0 else 0.0
             hist.append(rel)
@@ -371,16 +381,22 @@ class IcePhysics:
                 "lincomb")
         N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.z.data_ptr(), ntot, 1, s), "convert")
 
-    def adjoint(self, dL_du, dL_dv, dL_dH, n_vcycles=2, *, tol=None, max_vcycles=100, exact=False):
+    def adjoint(self, dL_du, dL_dv, dL_dH, n_vcycles=2, *, tol=None, max_vcycles=100, exact=False,
+                max_finish_sweeps=4000):
         """grad_beta of a loss through one implicit step (glide/physics.py:211-242).
 
         ``exact=True`` uses the exact transpose at clamped boundary reads in
         the VJP and the gradient (the reference drops some boundary terms).
-        With ``tol`` the adjoint cycles run until |f_adj - J^T lam| <= tol*|f_adj|.
+        With ``tol`` the adjoint cycles run until |f_adj - J_m^T lam| <=
+        tol |f_adj| (J_m: rows of cells at the thickness limit replaced by the
+        identity, as the adjoint smoother sees them); a cycle that cuts the
+        residual by less than ``stall_factor`` hands over to fine-level
+        adjoint sweeps.  ``last_adjoint_info`` records the work.
         """
         st = self.settings
         saved_exact = st.exact_adjoint
         st.exact_adjoint = bool(exact)
+        info = {"vcycles": 0, "finish_sweeps": 0, "rel_residual": None}
         try:
             g = self.grid
             g.f_adj_u.copy_(-_as_tensor(dL_du, g.dtype, self.device))
@@ -390,24 +406,41 @@ class IcePhysics:
             cfg = st.native(self.thklim)
             f0 = None
             n_max = max_vcycles if tol is not None else n_vcycles
+            prev = 1.0
+            rel = None
             for k in range(n_max):
                 if self.precision == "mixed":
                     self._adjoint_dc_step(cfg)
                 else:
                     N.check(self.kernels.glide_adjoint_vcycle(self._native, self._nlev, 0, C.byref(cfg),
                                                               N.stream_handle()), "adjoint_vcycle")
-                if tol is not None:
+                info["vcycles"] = k + 1
+                if tol is None:
+                    continue
+                rel, f0 = self._adjoint_rel(f0)
+                if rel <= tol or rel > self.stall_factor * prev:
+                    break
+                prev = rel
+            if tol is not None and rel is not None and rel > tol:
+                done = 0
+                while done < max_finish_sweeps and rel > tol and math.isfinite(rel):
+                    g.compute_mask()
+                    g.vanka_sweep_adjoint(self.finish_block, omega=st.adj_omega, exact_boundary=exact)
+                    g.mask.zero_()
+                    done += self.finish_block
                     rel, f0 = self._adjoint_rel(f0)
-                    if rel <= tol:
-                        break
+                info["finish_sweeps"] = done
+            info["rel_residual"] = rel
+            self.last_adjoint_info = info
             return g.compute_grad_beta(exact_boundary=exact)
         finally:
             st.exact_adjoint = saved_exact
 
     def _adjoint_rel(self, f0):
         g = self.grid
-        g.mask.zero_()
+        g.compute_mask()
         g.compute_adjoint_residual(self.settings.exact_adjoint)
+        g.mask.zero_()
         r = torch.sqrt(torch.sum(g.r_adj.double() ** 2)).item()
         if f0 is None:
             f0 = torch.sqrt(torch.sum(g.f_adj.double() ** 2)).item()

@@ -155,6 +155,25 @@ int glide_graph_create(GlideLevel* levels, int n_levels, const GlideSolverConfig
 int glide_graph_launch(void* graph, void* stream);
 int glide_graph_destroy(void* graph);
 
+/* ---- learned initial guess (no counterpart in the reference) -------------- */
+/* C[M,N] (+)= A[M,K] * B[N,K]^T on the tcgen05 tensor cores: A, B BF16 row-major
+ * with K contiguous (lda, ldb >= K, 16-byte aligned rows for the fast path),
+ * FP32 accumulation in TMEM; epilogue + bias[N] (may be null), ReLU if relu;
+ * out_mode 0 = store FP32, 1 = store BF16, 2 = add into FP32.  *err (may be
+ * null) is set to 1 if a tensor-core wait ran out (the tile is then skipped). */
+int glide_gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
+                    const float* bias, int relu, int out_mode, int* err, void* stream);
+/* im2col of a 3x3 same convolution on NHWC BF16 x (Bn,H,W,C) into col (Bn*H*W, Kp), Kp >= 9C (zero pad). */
+int glide_im2col3_bf16(const void* x, void* col, int Bn, int H, int W, int C, int Kp, void* stream);
+/* Transpose of im2col (gather form): dx (Bn,H,W,C) FP32 from dcol (Bn*H*W, Kp) FP32. */
+int glide_col2im3_f32(const float* dcol, float* dx, int Bn, int H, int W, int C, int Kp, void* stream);
+/* dst (Cc x R) = src (R x Cc)^T, BF16. */
+int glide_transpose_bf16(const void* src, void* dst, int R, int Cc, void* stream);
+
+/* Kernel launches issued by this library so far in the process (host-side
+ * count; launches recorded into a stream capture count once, at capture). */
+long long glide_launch_count(void);
+
 /* Library version string. */
 const char* glide_version(void);
 

@@ -1,0 +1,99 @@
+"""The hand-written VJP behind torch.autograd vs finite differences.
+
+Loss L = 1/2 |u - u_obs|^2 + 1/2 |v - v_obs|^2 with u_obs from a perturbed
+beta.  FP64, gl_derivatives on (so the JVP/VJP are the exact Jacobian),
+exact-boundary gradient, forward and adjoint solved to 1e-11.
+Central differences with eps = 1e-6 (relative to beta) on 16 seeded
+directions must agree with the adjoint directional derivative to 1e-5
+relative (the limit set by the solve tolerance over eps).
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+
+
+def _setup(n=32, seed=0):
+    from glide_b200 import IcePhysics, SolverSettings
+    from glide_b200.synthetic import dome_case
+    c = dome_case(seed, n=n, dx=5000.0 * 64 / n, n_levels=3)
+    ph = IcePhysics(n, n, c.dx, n_levels=3, thklim=c.thklim, precision="fp64", gl_derivatives=True,
+                    settings=SolverSettings(shift=0.0, err_threshold=1e-7), use_graphs=False)
+    ph.set_geometry(c.bed, c.thickness)
+    ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
+    beta = torch.as_tensor(c.beta, device="cuda")
+    H0 = torch.as_tensor(c.thickness, device="cuda")
+    return c, ph, beta, H0
+
+
+def _loss_fn(ph, H0, dt, u_obs, v_obs):
+    from glide_b200.adjoint import ssa_step
+
+    def L(beta):
+        u, v, H = ssa_step(beta, H0, ph, dt, tol=TOL, adj_tol=TOL)
+        return 0.5 * ((u - u_obs) ** 2).sum() + 0.5 * ((v - v_obs) ** 2).sum()
+    return L
+
+
+def test_step_gradient_matches_finite_differences():
+    from glide_b200.adjoint import ssa_step
+    c, ph, beta, H0 = _setup()
+    with torch.no_grad():
+        u_obs, v_obs, _ = ssa_step(beta * 1.3, H0, ph, c.dt, tol=TOL)
+        u_obs, v_obs = u_obs.clone(), v_obs.clone()
+    L = _loss_fn(ph, H0, c.dt, u_obs, v_obs)
+    b = beta.clone().requires_grad_(True)
+    loss = L(b)
+    loss.backward()
+    g = b.grad.clone()
+    rng = np.random.default_rng(16)
+    eps = 1e-6
+    errs = []
+    for k in range(16):
+        d = torch.as_tensor(rng.standard_normal(beta.shape), device="cuda") * beta
+        with torch.no_grad():
+            fd = (L(beta + eps * d) - L(beta - eps * d)) / (2 * eps)
+        ad = (g * d).sum()
+        errs.append(abs(float(fd - ad)) / max(abs(float(fd)), 1e-30))
+    assert max(errs) <= 1e-5, errs
+
+
+def test_gradcheck_fast_mode():
+    """torch.autograd.gradcheck (random-projection mode) on the step function."""
+    from glide_b200.adjoint import ssa_step
+    c, ph, beta, H0 = _setup(n=16)
+    u_obs = torch.zeros(16, 17, dtype=torch.float64, device="cuda")
+    v_obs = torch.zeros(17, 16, dtype=torch.float64, device="cuda")
+
+    def f(b, h):
+        u, v, H = ssa_step(b, h, ph, c.dt, tol=TOL, adj_tol=TOL)
+        return 0.5 * ((u - u_obs) ** 2).sum() + 0.5 * ((v - v_obs) ** 2).sum()
+
+    b = beta.clone().requires_grad_(True)
+    h = H0.clone().requires_grad_(True)
+    assert torch.autograd.gradcheck(f, (b, h), eps=1e-6, atol=1e-6, rtol=1e-4, fast_mode=True)
+
+
+def test_time_stepped_checkpointed_gradient():
+    """4 steps, checkpoint every 2: gradient w.r.t. beta vs central differences."""
+    from glide_b200.adjoint import time_stepped
+    c, ph, beta, H0 = _setup(n=32, seed=1)
+
+    def L(b):
+        u, v, H = time_stepped(b, H0, ph, c.dt, n_steps=4, checkpoint_every=2, tol=TOL, adj_tol=TOL)
+        return 0.5 * (u ** 2).sum() + 0.5 * (v ** 2).sum() + 1e-3 * (H ** 2).sum()
+
+    b = beta.clone().requires_grad_(True)
+    L(b).backward()
+    g = b.grad.clone()
+    rng = np.random.default_rng(4)
+    eps = 1e-6
+    for k in range(3):
+        d = torch.as_tensor(rng.standard_normal(beta.shape), device="cuda") * beta
+        with torch.no_grad():
+            fd = (L(beta + eps * d) - L(beta - eps * d)) / (2 * eps)
+        ad = (g * d).sum()
+        assert abs(float(fd - ad)) <= 1e-4 * abs(float(fd))
