@@ -22,7 +22,8 @@ SYMBOLS = [
     "glide_tile_flags", "glide_vanka_adjoint", "glide_restrict", "glide_prolong", "glide_lincomb", "glide_fill",
     "glide_mask_le", "glide_convert", "glide_norms", "glide_norm_parts", "glide_fascd_vcycle",
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
-    "glide_graph_destroy", "glide_launch_count", "glide_version",
+    "glide_graph_destroy", "glide_launch_count", "glide_version", "glide_vanka_sweeps_noalloc",
+    "glide_noalloc_scratch_bytes",
 ]
 
 
@@ -99,12 +100,15 @@ def load():
         "glide_graph_launch": [vp, vp],
         "glide_graph_destroy": [vp],
         "glide_launch_count": [],
+        "glide_vanka_sweeps_noalloc": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp],
+        "glide_noalloc_scratch_bytes": [],
         "glide_version": [],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
-        f.restype = C.c_char_p if name == "glide_version" else (C.c_longlong if name == "glide_launch_count" else C.c_int)
+        f.restype = {"glide_version": C.c_char_p, "glide_launch_count": C.c_longlong,
+                     "glide_noalloc_scratch_bytes": C.c_size_t}.get(name, C.c_int)
     _lib = lib
     return lib
 

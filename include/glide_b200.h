@@ -30,6 +30,7 @@
 #ifndef GLIDE_B200_H
 #define GLIDE_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -44,6 +45,7 @@ extern "C" {
 #define GLIDE_E_SHAPE (-2)
 #define GLIDE_E_NULL (-3)
 #define GLIDE_E_GRAPH (-4)
+#define GLIDE_E_TOO_LARGE (-5)
 
 typedef struct GlidePhysicsParams {
     double n;             /* Glen exponent */
@@ -84,6 +86,18 @@ int glide_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, v
 int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                        int n_newton, double omega, double shift, const int* flags, const int* any_active,
                        void* scratch, void* stream);
+/* Same sweeps as glide_vanka_sweeps for callers that cannot allocate device
+ * memory (no counterpart in the reference): the scratch lives in a fixed
+ * 10 MiB device array inside the library (glide_noalloc_scratch_bytes()),
+ * enough for nb*ny*nx <= 262144 cells in FP64 or 524288 in FP32; larger
+ * problems return GLIDE_E_TOO_LARGE.  The first call on a device (with that
+ * device current) looks up the array's device address; make it before any
+ * stream capture.  All calls share the array, so calls that overlap on the
+ * GPU race and must be ordered by the caller.  Allocates nothing. */
+int glide_vanka_sweeps_noalloc(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
+                               int n_newton, double omega, double shift, const int* flags, const int* any_active,
+                               void* stream);
+size_t glide_noalloc_scratch_bytes(void);
 /* Only the per-cell local Newton kernel of a sweep, n_launch times, writing the
  * per-cell deltas into scratch without updating U (profiling and timing). */
 int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,

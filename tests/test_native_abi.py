@@ -16,7 +16,7 @@ def _declared():
     names = set()
     for h in (ROOT / "include").glob("*.h"):
         txt = h.read_text()
-        for m in re.finditer(r"^\s*(?:int|const char\*)\s+(glide_\w+)\s*\(", txt, re.M):
+        for m in re.finditer(r"^\s*(?:int|const char\*|long long|size_t)\s+(glide_\w+)\s*\(", txt, re.M):
             names.add(m.group(1))
     return sorted(names)
 
