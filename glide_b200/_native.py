@@ -23,7 +23,7 @@ SYMBOLS = [
     "glide_mask_le", "glide_convert", "glide_norms", "glide_norm_parts", "glide_fascd_vcycle",
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
     "glide_graph_destroy", "glide_launch_count", "glide_version", "glide_vanka_sweeps_noalloc",
-    "glide_noalloc_scratch_bytes",
+    "glide_noalloc_scratch_bytes", "glide_vanka_sweeps_ex",
 ]
 
 
@@ -54,7 +54,8 @@ class SolverConfig(C.Structure):
     _fields_ = [("thklim", C.c_double), ("n_coarse", C.c_int), ("n_smooth", C.c_int), ("n_local_outer", C.c_int),
                 ("n_local", C.c_int), ("n_newton", C.c_int), ("omega", C.c_double), ("shift", C.c_double),
                 ("err_threshold", C.c_double), ("adj_coarse", C.c_int), ("adj_smooth", C.c_int),
-                ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int)]
+                ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int),
+                ("newton_step", C.c_double)]
 
 
 class NativeError(RuntimeError):
@@ -81,6 +82,7 @@ def load():
         "glide_vjp": [LA, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp],
         "glide_grad_beta": [LA, vp, vp, vp, i, vp],
         "glide_vanka_sweeps": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp, vp],
+        "glide_vanka_sweeps_ex": [LA, vp, vp, vp, i, i, d, d, d, vp, vp, vp, vp],
         "glide_vanka_cells": [LA, vp, vp, vp, i, i, d, vp, vp, vp, vp],
         "glide_error_mask": [LA, vp, vp, vp, d, vp, vp, vp, vp],
         "glide_tile_flags": [LA, vp, vp, vp, vp],

@@ -20,8 +20,8 @@ template <typename T> int launch_residual(const GlideLevelArgs*, const void*, co
 template <typename T> int launch_jvp(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*, cudaStream_t);
 template <typename T> int launch_vjp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*, void*, void*, void*, int, cudaStream_t);
 template <typename T> int launch_grad_beta(const GlideLevelArgs*, const void*, const void*, void*, int, cudaStream_t);
-template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t);
-template <typename T> int launch_vanka_cells(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, const int*, const int*, void*, cudaStream_t);
+template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t, double);
+template <typename T> int launch_vanka_cells(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, const int*, const int*, void*, cudaStream_t, double);
 template <typename T> int launch_error_mask(const GlideLevelArgs*, const void*, const void*, const void*, double, void*, int*, int*, cudaStream_t);
 template <typename T> int launch_tile_flags(const GlideLevelArgs*, const void*, int*, int*, cudaStream_t);
 template <typename T> int launch_vanka_adjoint(const GlideLevelArgs*, void*, void*, void*, const void*, const void*, const void*, int, double, cudaStream_t);
@@ -102,19 +102,26 @@ int glide_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, v
                      launch_grad_beta<double>(a, l_u, l_v, grad, exact_boundary, S(stream)));
 }
 
-int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
-                       int n_newton, double omega, double shift, const int* flags, const int* any_active,
-                       void* scratch, void* stream) {
+int glide_vanka_sweeps_ex(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
+                          int n_newton, double newton_step, double omega, double shift, const int* flags,
+                          const int* any_active, void* scratch, void* stream) {
     int e = check_level(a);
     if (e) return e;
     if (!f_u || !f_v || !f_H || !scratch) return GLIDE_E_NULL;
     if ((flags == nullptr) != (any_active == nullptr)) return GLIDE_E_NULL;
-    if (n_iter < 0 || n_newton < 0) return GLIDE_E_SHAPE;
+    if (n_iter < 0 || n_newton < 0 || !(newton_step > 0.0 && newton_step <= 1.0)) return GLIDE_E_SHAPE;
     return TDISPATCH(a->dtype,
                      launch_vanka_sweeps<float>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags, any_active,
-                                                scratch, S(stream)),
+                                                scratch, S(stream), newton_step),
                      launch_vanka_sweeps<double>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags,
-                                                 any_active, scratch, S(stream)));
+                                                 any_active, scratch, S(stream), newton_step));
+}
+
+int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
+                       int n_newton, double omega, double shift, const int* flags, const int* any_active,
+                       void* scratch, void* stream) {
+    return glide_vanka_sweeps_ex(a, f_u, f_v, f_H, n_iter, n_newton, GLIDE_REF_NEWTON_STEP, omega, shift, flags,
+                                 any_active, scratch, stream);
 }
 
 int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,
@@ -127,9 +134,9 @@ int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v,
     if (n_launch < 0 || n_newton < 0) return GLIDE_E_SHAPE;
     return TDISPATCH(a->dtype,
                      launch_vanka_cells<float>(a, f_u, f_v, f_H, n_launch, n_newton, shift, flags, any_active,
-                                               scratch, S(stream)),
+                                               scratch, S(stream), GLIDE_REF_NEWTON_STEP),
                      launch_vanka_cells<double>(a, f_u, f_v, f_H, n_launch, n_newton, shift, flags, any_active,
-                                                scratch, S(stream)));
+                                                scratch, S(stream), GLIDE_REF_NEWTON_STEP));
 }
 
 int glide_error_mask(const GlideLevelArgs* a, const void* r_u, const void* r_v, const void* r_H, double threshold,
@@ -261,8 +268,9 @@ LevelView view(GlideLevel* L) {
 
 int vanka(GlideLevel* L, int n_iter, const GlideSolverConfig* c, bool local, void* s) {
     LevelView w = view(L);
-    return glide_vanka_sweeps(&L->a, w.u(L->f), w.v(L->f), w.H(L->f), n_iter, c->n_newton, c->omega, c->shift,
-                              local ? L->flags : nullptr, local ? L->any_active : nullptr, L->scratch, s);
+    const double step = c->newton_step > 0.0 ? c->newton_step : GLIDE_REF_NEWTON_STEP;
+    return glide_vanka_sweeps_ex(&L->a, w.u(L->f), w.v(L->f), w.H(L->f), n_iter, c->n_newton, step, c->omega,
+                                 c->shift, local ? L->flags : nullptr, local ? L->any_active : nullptr, L->scratch, s);
 }
 
 int fill_gamma(GlideLevel* L, double val, void* s) {

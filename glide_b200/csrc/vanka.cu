@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : 1) vanka_cells_kerne
     T* __restrict__ scratch, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, const T* __restrict__ bed,
     const T* __restrict__ B, const T* __restrict__ beta, const T* __restrict__ gamma, const int* __restrict__ flags,
-    const int* __restrict__ any_active, int n_newton, T shift, Geo g, Phys<T> p) {
+    const int* __restrict__ any_active, int n_newton, T shift, T step, Geo g, Phys<T> p) {
     __shared__ T s_eta[VY + 2][VX + 2];
     const int ny = g.ny, nx = g.nx;
     const int bz = blockIdx.z;
@@ -458,11 +458,11 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : 1) vanka_cells_kerne
         assemble_fast<T>(F, ul, ur, vt, vb, Hc, fu_l, fu_r, fv_t, fv_b, fH, thk, dti, p, J, rr);
         J[0] -= shift; J[6] -= shift; J[12] -= shift; J[18] -= shift; J[24] += shift;  // vanka.cu:406-410
         lu5_solve_fast(J, rr, x);
-        ul -= T(0.25) * x[0];
-        ur -= T(0.25) * x[1];
-        vt -= T(0.25) * x[2];
-        vb -= T(0.25) * x[3];
-        Hc -= T(0.25) * x[4];
+        ul -= step * x[0];  // reference step 0.25: relaxation_factor, glide/cuda/vanka.cu:416
+        ur -= step * x[1];
+        vt -= step * x[2];
+        vb -= step * x[3];
+        Hc -= step * x[4];
         Hc = M<T>::max(Hc, thk);
     }
     const int64_t ic = int64_t(i) * nx + j;
@@ -604,7 +604,7 @@ static inline dim3 face_grid(const Geo& g) { return dim3((g.nx + 1 + 31) / 32, (
 template <typename T>
 int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                         int n_newton, double omega, double shift, const int* flags, const int* any_active,
-                        void* scratch, cudaStream_t s) {
+                        void* scratch, cudaStream_t s, double newton_step) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     T* u = (T*)a->u;
@@ -614,13 +614,13 @@ int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_
         if (flags) {
             glide::count_launch(), vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, u, v, H, (const T*)f_u, (const T*)f_v, (const T*)f_H, (const T*)a->bed,
-                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags, any_active, n_newton, T(shift), g, p);
+                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags, any_active, n_newton, T(shift), T(newton_step), g, p);
             glide::count_launch(), vanka_apply_kernel<T, true><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, flags,
                                                                                any_active, T(omega), g);
         } else {
             glide::count_launch(), vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, u, v, H, (const T*)f_u, (const T*)f_v, (const T*)f_H, (const T*)a->bed,
-                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr, nullptr, n_newton, T(shift), g, p);
+                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr, nullptr, n_newton, T(shift), T(newton_step), g, p);
             glide::count_launch(), vanka_apply_kernel<T, false><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, nullptr,
                                                                                 nullptr, T(omega), g);
         }
@@ -632,7 +632,7 @@ int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_
 template <typename T>
 int launch_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,
                        int n_newton, double shift, const int* flags, const int* any_active, void* scratch,
-                       cudaStream_t s) {
+                       cudaStream_t s, double newton_step) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     for (int k = 0; k < n_launch; k++) {
@@ -640,12 +640,12 @@ int launch_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v
             glide::count_launch(), vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
                 (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags,
-                any_active, n_newton, T(shift), g, p);
+                any_active, n_newton, T(shift), T(newton_step), g, p);
         else
             glide::count_launch(), vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
                 (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr,
-                nullptr, n_newton, T(shift), g, p);
+                nullptr, n_newton, T(shift), T(newton_step), g, p);
     }
     return (int)cudaGetLastError();
 }
@@ -689,9 +689,9 @@ int launch_vanka_adjoint(const GlideLevelArgs* a, void* l_u, void* l_v, void* l_
 
 #define INST(T)                                                                                                  \
     template int launch_vanka_sweeps<T>(const GlideLevelArgs*, const void*, const void*, const void*, int, int,   \
-                                        double, double, const int*, const int*, void*, cudaStream_t);             \
+                                        double, double, const int*, const int*, void*, cudaStream_t, double);     \
     template int launch_vanka_cells<T>(const GlideLevelArgs*, const void*, const void*, const void*, int, int,     \
-                                       double, const int*, const int*, void*, cudaStream_t);                      \
+                                       double, const int*, const int*, void*, cudaStream_t, double);              \
     template int launch_error_mask<T>(const GlideLevelArgs*, const void*, const void*, const void*, double,       \
                                       void*, int*, int*, cudaStream_t);                                           \
     template int launch_tile_flags<T>(const GlideLevelArgs*, const void*, int*, int*, cudaStream_t);              \

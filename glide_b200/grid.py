@@ -158,14 +158,14 @@ class Grid:
                                     self.lambda_H.data_ptr(), None, None, None, self.l_u.data_ptr(),
                                     self.l_v.data_ptr(), self.l_H.data_ptr(), int(exact_boundary), self._s()), "vjp")
 
-    def _sweeps(self, n_iter, n_inner, omega, shift, local):
+    def _sweeps(self, n_iter, n_inner, omega, shift, local, step=0.25):
         a = self.level_args()
         flags = self._flags.data_ptr() if local else None
         anyact = self._any_active.data_ptr() if local else None
-        N.check(self._lib.glide_vanka_sweeps(C.byref(a), self.f_u.data_ptr(), self.f_v.data_ptr(),
-                                             self.f_H.data_ptr(), int(n_iter), int(n_inner), float(omega),
-                                             float(shift), flags, anyact, self._scratch.data_ptr(), self._s()),
-                "vanka")
+        N.check(self._lib.glide_vanka_sweeps_ex(C.byref(a), self.f_u.data_ptr(), self.f_v.data_ptr(),
+                                                self.f_H.data_ptr(), int(n_iter), int(n_inner), float(step),
+                                                float(omega), float(shift), flags, anyact, self._scratch.data_ptr(),
+                                                self._s()), "vanka")
 
     def vanka_smooth(self, color=0, omega=1.0, n_inner=1, shift=1.0):
         """One ``vanka_smooth`` launch: adds the face/cell deltas into
@@ -188,14 +188,15 @@ class Grid:
         N.check(self._lib.glide_tile_flags(C.byref(a), self.error_mask.data_ptr(), self._flags.data_ptr(),
                                            self._any_active.data_ptr(), self._s()), "tile flags")
 
-    def vanka_sweep(self, n_iter, n_inner=10, omega=0.5, shift=1.0):
-        """n_iter sweeps with U += omega*delta (glide/grid.py:305-310)."""
-        self._sweeps(n_iter, n_inner, omega, shift, False)
+    def vanka_sweep(self, n_iter, n_inner=10, omega=0.5, shift=1.0, step=0.25):
+        """n_iter sweeps with U += omega*delta (glide/grid.py:305-310); ``step``
+        is the local Newton step fraction (reference 0.25)."""
+        self._sweeps(n_iter, n_inner, omega, shift, False, step)
 
-    def vanka_sweep_local(self, n_iter, n_inner=10, omega=0.5, shift=1.0):
+    def vanka_sweep_local(self, n_iter, n_inner=10, omega=0.5, shift=1.0, step=0.25):
         """Sweeps gated by error_mask (glide/grid.py:312-317)."""
         self.update_tile_flags()
-        self._sweeps(n_iter, n_inner, omega, shift, True)
+        self._sweeps(n_iter, n_inner, omega, shift, True, step)
 
     def vanka_smooth_adjoint(self, color, omega=0.5):
         """One adjoint colour update from the current r_adj (glide/grid.py:286-303)."""

@@ -60,7 +60,8 @@ class IcePhysics:
     def __init__(self, ny, nx, dx, n_levels=5, n=3.0, eps_reg=1e-5, thklim=0.1, water_drag=1e-3, calving_rate=1.0,
                  gl_sigmoid_c=0.1, gl_derivatives=False, *, precision="fp32", device=None,
                  settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0,
-                 stall_factor=0.5, finish_block=20, finish_anderson=0, finish_fp32=False):
+                 stall_factor=0.5, finish_block=20, finish_anderson=0, finish_fp32=False, finish_newton=None,
+                 finish_step=None):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -80,6 +81,8 @@ class IcePhysics:
         self.finish_block = int(finish_block)
         self.finish_anderson = int(finish_anderson)
         self.finish_fp32 = bool(finish_fp32)
+        self.finish_newton = None if finish_newton is None else int(finish_newton)
+        self.finish_step = None if finish_step is None else float(finish_step)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
         self.dtype = _PRECISIONS[precision]
@@ -330,7 +333,7 @@ class IcePhysics:
             if use32:
                 self._fp32_sweeps(self.finish_block)
             else:
-                g.vanka_sweep(self.finish_block, n_inner=st.n_newton, omega=st.omega, shift=st.shift)
+                g.vanka_sweep(self.finish_block, omega=st.omega, shift=st.shift, **self._finish_local())
             done += self.finish_block
             if m > 0:
                 Gx = g.U[:nU].clone()
@@ -361,6 +364,13 @@ class IcePhysics:
         info["finish_sweeps"] = done
         return rel
 
+    def _finish_local(self):
+        """Local Newton iterations and step fraction of the finishing sweeps
+        (``finish_newton``/``finish_step``; default: the cycle's settings)."""
+        st = self.settings
+        return dict(n_inner=st.n_newton if self.finish_newton is None else self.finish_newton,
+                    step=st.newton_step if self.finish_step is None else self.finish_step)
+
     def _fp32_sweeps(self, n):
         """FP32 fine-level sweeps on the FP64 problem's correction equation."""
         g64, g32 = self.grid, self.grid32
@@ -376,7 +386,7 @@ class IcePhysics:
         a = g32.level_args()
         N.check(lib.glide_residual(C.byref(a), g32.r_u.data_ptr(), g32.r_v.data_ptr(), g32.r_H.data_ptr(),
                                    g32.f_u.data_ptr(), g32.f_v.data_ptr(), g32.f_H.data_ptr(), s), "residual32")
-        g32.vanka_sweep(n, n_inner=st.n_newton, omega=st.omega, shift=st.shift)
+        g32.vanka_sweep(n, omega=st.omega, shift=st.shift, **self._finish_local())
         N.check(lib.glide_lincomb(N.F32, g32.z.data_ptr(), g32.U.data_ptr(), 1.0, g32.w.data_ptr(), -1.0, ntot, s),
                 "lincomb")
         N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.z.data_ptr(), ntot, 1, s), "convert")

@@ -32,6 +32,7 @@ class SolverSettings:
     adj_omega: float = 1.0
     exact_adjoint: bool = False  # reference VJP/grad boundary handling when False
     smooth_H_correction: bool = False  # bilinear instead of injected coarse H correction
+    newton_step: float = 0.25  # fraction of each local Newton step (relaxation_factor, glide/cuda/vanka.cu:416)
 
     def native(self, thklim) -> N.SolverConfig:
         c = N.SolverConfig()
@@ -42,6 +43,7 @@ class SolverSettings:
         c.adj_coarse, c.adj_smooth, c.adj_omega = self.adj_coarse, self.adj_smooth, float(self.adj_omega)
         c.exact_adjoint = int(self.exact_adjoint)
         c.smooth_H_correction = int(self.smooth_H_correction)
+        c.newton_step = float(self.newton_step)
         return c
 
 

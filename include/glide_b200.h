@@ -47,6 +47,10 @@ extern "C" {
 #define GLIDE_E_GRAPH (-4)
 #define GLIDE_E_TOO_LARGE (-5)
 
+/* Fraction of each local Newton step the reference's Vanka smoother takes
+ * (relaxation_factor, glide/cuda/vanka.cu:416). */
+#define GLIDE_REF_NEWTON_STEP 0.25
+
 typedef struct GlidePhysicsParams {
     double n;             /* Glen exponent */
     double eps_reg;       /* strain-rate regularisation */
@@ -86,6 +90,13 @@ int glide_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, v
 int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                        int n_newton, double omega, double shift, const int* flags, const int* any_active,
                        void* scratch, void* stream);
+/* glide_vanka_sweeps with the local Newton step fraction as an argument
+ * (0 < newton_step <= 1; the reference fixes it at GLIDE_REF_NEWTON_STEP).
+ * Extension, no counterpart in the reference: the tolerance solver's
+ * finishing sweeps take full local Newton steps with few iterations. */
+int glide_vanka_sweeps_ex(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
+                          int n_newton, double newton_step, double omega, double shift, const int* flags,
+                          const int* any_active, void* scratch, void* stream);
 /* Same sweeps as glide_vanka_sweeps for callers that cannot allocate device
  * memory (no counterpart in the reference): the scratch lives in a fixed
  * 10 MiB device array inside the library (glide_noalloc_scratch_bytes()),
@@ -154,6 +165,8 @@ typedef struct GlideSolverConfig {
     double adj_omega;
     int exact_adjoint;      /* 0: reference VJP boundary handling */
     int smooth_H_correction;/* 0: inject the coarse H correction (reference), 1: bilinear */
+    double newton_step;     /* fraction of each local Newton step taken in the forward sweeps;
+                               <= 0 means the reference's GLIDE_REF_NEWTON_STEP */
 } GlideSolverConfig;
 
 /* One FASCD V-cycle from level k0 (finest=1 sets w=U, chi=gamma-H first). */

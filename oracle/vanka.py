@@ -245,7 +245,7 @@ def _assemble(fz: _Frozen, ul, ur, vt, vb, Hc, p: Params, dx, dt, with_res, f=No
 
 
 def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt, n_newton=10, cell_on=None,
-                 shift=1.0, return_cells=False):
+                 shift=1.0, return_cells=False, step=0.25):
     """Delta arrays written by one ``vanka_smooth`` launch (vanka.cu:3-439).
 
     Each cell runs ``n_newton`` damped (0.25) Newton steps on its 5 unknowns
@@ -254,7 +254,9 @@ def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt,
     (vanka.cu:423).  Faces receive 0.5*(change) from each adjacent cell
     (vanka.cu:433-436), H the full change.  ``cell_on`` (bool (ny,nx))
     restricts the update to those cells, as the block gating of
-    ``vanka_smooth_local`` does.
+    ``vanka_smooth_local`` does.  ``step`` is the Newton step fraction
+    (0.25 = relaxation_factor, vanka.cu:416; other values test the
+    extension entry point glide_vanka_sweeps_ex).
     """
     ny, nx = H.shape
     fz = _Frozen(u, v, H, bed, B, beta, p, dx)
@@ -266,11 +268,11 @@ def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt,
         Jm, r = _assemble(fz, ul, ur, vt, vb, Hc, p, dx, dt, True, (f_u, f_v, f_H), thklim)
         Jm[0] -= shift; Jm[6] -= shift; Jm[12] -= shift; Jm[18] -= shift; Jm[24] += shift
         x = lu5_solve(Jm, r)
-        ul = ul - 0.25 * x[0]
-        ur = ur - 0.25 * x[1]
-        vt = vt - 0.25 * x[2]
-        vb = vb - 0.25 * x[3]
-        Hc = Hc - 0.25 * x[4]
+        ul = ul - step * x[0]
+        ur = ur - step * x[1]
+        vt = vt - step * x[2]
+        vb = vb - step * x[3]
+        Hc = Hc - step * x[4]
         Hc = np.maximum(Hc, thklim)
     on = np.ones((ny, nx), bool) if cell_on is None else cell_on
     d_ul = np.where(on, 0.5 * (ul - ul0), 0.0)

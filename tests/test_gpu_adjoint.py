@@ -78,22 +78,36 @@ def test_gradcheck_fast_mode():
 
 
 def test_time_stepped_checkpointed_gradient():
-    """4 steps, checkpoint every 2: gradient w.r.t. beta vs central differences."""
-    from glide_b200.adjoint import time_stepped
-    c, ph, beta, H0 = _setup(n=32, seed=1)
+    """4 steps: the gradient w.r.t. beta is identical for checkpoint spacings
+    1, 2 and 4 (recomputation replays the same solves), and agrees with
+    central differences to 1e-4 relative on 3 seeded directions.
 
-    def L(b):
-        u, v, H = time_stepped(b, H0, ph, c.dt, n_steps=4, checkpoint_every=2, tol=TOL, adj_tol=TOL)
+    The differences are taken where the step map is smooth: central
+    differences at eps and 2*eps must agree first.  (The dome of seed 1 at
+    dt = 10 a has a bistable margin cell, index (26, 7): a 1e-6 relative
+    change of beta moves its thickness by ~150 m onto another solution
+    branch; the FP64 NumPy oracle finds the same two branches.)"""
+    from glide_b200.adjoint import time_stepped
+    c, ph, beta, H0 = _setup(n=32, seed=0)
+
+    def L(b, every=2):
+        u, v, H = time_stepped(b, H0, ph, c.dt, n_steps=4, checkpoint_every=every, tol=TOL, adj_tol=TOL)
         return 0.5 * (u ** 2).sum() + 0.5 * (v ** 2).sum() + 1e-3 * (H ** 2).sum()
 
-    b = beta.clone().requires_grad_(True)
-    L(b).backward()
-    g = b.grad.clone()
+    grads = []
+    for every in (2, 1, 4):
+        b = beta.clone().requires_grad_(True)
+        L(b, every).backward()
+        grads.append(b.grad.clone())
+    for other in grads[1:]:
+        assert torch.equal(other, grads[0])
+    g = grads[0]
     rng = np.random.default_rng(4)
-    eps = 1e-6
     for k in range(3):
         d = torch.as_tensor(rng.standard_normal(beta.shape), device="cuda") * beta
         with torch.no_grad():
-            fd = (L(beta + eps * d) - L(beta - eps * d)) / (2 * eps)
-        ad = (g * d).sum()
-        assert abs(float(fd - ad)) <= 1e-4 * abs(float(fd))
+            fd = ((L(beta + 1e-6 * d) - L(beta - 1e-6 * d)) / 2e-6).item()
+            fd2 = ((L(beta + 2e-6 * d) - L(beta - 2e-6 * d)) / 4e-6).item()
+        assert abs(fd2 - fd) <= 1e-4 * abs(fd), "finite differences cross a solution branch"
+        ad = (g * d).sum().item()
+        assert abs(fd - ad) <= 1e-4 * abs(fd), (k, fd, ad)

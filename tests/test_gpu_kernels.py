@@ -8,6 +8,7 @@ and a batch of 3 problems.
 """
 import numpy as np
 import pytest
+import torch
 
 from conftest import random_state
 
@@ -131,19 +132,37 @@ def test_grad_beta(precision, exact):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("shift", [1.0, 0.0])
-def test_vanka_sweep(precision, shift):
+@pytest.mark.parametrize("shift,step,n_newton", [(1.0, 0.25, 10), (0.0, 0.25, 10), (0.0, 1.0, 2)])
+def test_vanka_sweep(precision, shift, step, n_newton):
+    """One sweep vs the oracle; step 0.25 is the reference smoother, step 1.0
+    with 2 iterations the finishing sweeps of the tolerance solver."""
     from oracle.vanka import vanka_deltas
     st = _state((32, 32), seed=5)
     st["u"] *= 0.02
     st["v"] *= 0.02
     g = _grid(st, precision)
-    g.vanka_sweep(1, n_inner=10, omega=0.5, shift=shift)
+    g.vanka_sweep(1, n_inner=n_newton, omega=0.5, shift=shift, step=step)
     du, dv, dH = vanka_deltas(st["u"], st["v"], st["H"], st["f_u"], st["f_v"], st["f_H"], st["bed"], st["B"],
-                              st["beta"], st["gamma"], _params(), st["dx"], st["dt"], 10, shift=shift)
+                              st["beta"], st["gamma"], _params(), st["dx"], st["dt"], n_newton, shift=shift, step=step)
     tol = TOL[precision] * (1 if precision == "fp64" else 20)
     for a, x0, d in zip((g.u, g.v, g.H), (st["u"], st["v"], st["H"]), (du, dv, dH)):
         assert _rel(_np(a) - x0, 0.5 * d) <= tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vanka_ex_reference_step_is_the_reference_entry_point(precision):
+    """glide_vanka_sweeps_ex with step 0.25 is bit-identical to glide_vanka_sweeps."""
+    import ctypes as C
+    st = _state((40, 24), seed=6)
+    st["u"] *= 0.02
+    st["v"] *= 0.02
+    a, b = _grid(st, precision), _grid(st, precision)
+    a.vanka_sweep(2, n_inner=10, omega=0.5, shift=1.0)
+    args = b.level_args()
+    rc = b._lib.glide_vanka_sweeps(C.byref(args), b.f_u.data_ptr(), b.f_v.data_ptr(), b.f_H.data_ptr(), 2, 10, 0.5,
+                                   1.0, None, None, b._scratch.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    assert torch.equal(a.U, b.U)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])

@@ -51,8 +51,12 @@ def test_noalloc_matches_allocating_sweeps_twice(dtype):
     st = random_state(n=48, seed=31)
     a_grid, b_grid = _grid(st, dtype), _grid(st, dtype)
     s = torch.cuda.current_stream().cuda_stream
+    scratch = torch.empty(5 * 48 * 48, dtype=dtype, device="cuda")   # the allocating entry point's scratch
     for call in range(2):
-        a_grid.vanka_sweep(3, n_inner=10, omega=0.5, shift=1.0)          # allocating entry point
+        a_args = a_grid.level_args()
+        rc = lib.glide_vanka_sweeps(C.byref(a_args), a_grid.f_u.data_ptr(), a_grid.f_v.data_ptr(),
+                                    a_grid.f_H.data_ptr(), 3, 10, 0.5, 1.0, None, None, scratch.data_ptr(), s)
+        assert rc == 0
         args = b_grid.level_args()
         rc = lib.glide_vanka_sweeps_noalloc(C.byref(args), b_grid.f_u.data_ptr(), b_grid.f_v.data_ptr(),
                                             b_grid.f_H.data_ptr(), 3, 10, 0.5, 1.0, None, None, s)
