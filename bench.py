@@ -10,14 +10,17 @@ inputs stand in for the reference's datasets (no network here).
 Arms
   (default)          this package on N GPUs, one process per GPU (replicas:
                      every rank solves its own geometries, no collective in the
-                     data path; scaling "weak").  ``value`` is the fast path
-                     (FP32 V-cycles + FP64 defect correction, learned initial
-                     guess when a trained model is available); the plain FP64
-                     FAS path is reported beside it.
-  --impl reference   the reference discretisation in FP64 NumPy on the host
-                     cores (the reference itself is GPU-only), timed on a
-                     bounded sample: full-size fine-level Vanka sweeps, scaled
-                     to a step by the cycle structure.
+                     data path; scaling "weak").  ``value`` is the fast path:
+                     FP32 V-cycles with FP64 defect correction, full-step local
+                     Newton (2 iterations) in the smoother, FP32/FP64
+                     finishing sweeps with Anderson acceleration.  Beside it:
+                     the same path started from the learned initial guess
+                     (``learned_guess``), and the plain FP64 FAS path with the
+                     reference's smoother (``plain_fp64_fas``).
+  --impl reference   the plain FAS algorithm in FP64 NumPy on the host cores
+                     (the reference itself is GPU-only), timed on a bounded
+                     sample: full-size fine-level Vanka sweeps, scaled to a
+                     step by the plain path's cycle and sweep counts.
 
 Prints one JSON line on rank 0.
 """
@@ -52,6 +55,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--max-vcycles", type=int, default=40)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 FAS comparison arm")
+    ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     return ap.parse_args()
 
@@ -150,9 +154,20 @@ def max_over_ranks(x, world):
 # our arm
 # ---------------------------------------------------------------------------
 def tol_settings():
-    """Solver settings used to reach the tolerance (both arms of the comparison)."""
+    """Plain FAS: the reference's smoother (10 local Newton iterations, step
+    0.25, 10 local rounds) without the diagonal shift and with a small local
+    threshold, so that the tolerance is reachable."""
     from glide_b200.solver import SolverSettings
     return SolverSettings(shift=0.0, err_threshold=1e-7)
+
+
+def fast_settings():
+    """Fast path: 2 full local Newton steps per cell, 2 local rounds."""
+    from glide_b200.solver import SolverSettings
+    return SolverSettings(shift=0.0, err_threshold=1e-7, n_local_outer=2, n_newton=2, newton_step=1.0)
+
+
+FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0)
 
 
 def make_cases(n, seeds):
@@ -163,11 +178,11 @@ def make_cases(n, seeds):
 class Runner:
     """Solves fresh geometries with one IcePhysics instance."""
 
-    def __init__(self, n, precision, guess_model=None, max_vcycles=40):
+    def __init__(self, n, precision, guess_model=None, max_vcycles=40, settings=None, **kw):
         import torch
         from glide_b200 import IcePhysics
         self.ph = IcePhysics(n, n, DX * 1024 / n, n_levels=LEVELS, thklim=0.1, precision=precision,
-                             settings=tol_settings())
+                             settings=settings or tol_settings(), **kw)
         self.guess_model = guess_model
         self.max_vcycles = max_vcycles
         self.torch = torch
@@ -238,7 +253,8 @@ def dominant_kernel_timing(runner, sweeps=20):
     saved = g.U.clone()
     torch.cuda.synchronize()
     ev[0].record(s)
-    N.check(lib.glide_vanka_cells(C.byref(a), g.f_u.data_ptr(), g.f_v.data_ptr(), g.f_H.data_ptr(), sweeps, 10,
+    N.check(lib.glide_vanka_cells(C.byref(a), g.f_u.data_ptr(), g.f_v.data_ptr(), g.f_H.data_ptr(), sweeps,
+                                  ph.settings.n_newton,
                                   float(ph.settings.shift), None, None, g._scratch.data_ptr(), s.cuda_stream),
             "vanka cells")
     ev[1].record(s)
@@ -264,9 +280,9 @@ def run_ours(args):
     try:
         from glide_b200.guess import load_default_model
         guess_model = load_default_model()
-    except Exception:
-        guess_model = None
-    fast = Runner(n, "mixed", guess_model, args.max_vcycles)
+    except Exception as e:  # the learned-guess arm is reported as unavailable
+        print(f"learned guess unavailable: {e}", file=sys.stderr)
+    fast = Runner(n, "mixed", None, args.max_vcycles, fast_settings(), **FAST_KW)
     fdev = [fast.load_device(c) for c in cases]
 
     sampler = ClockSampler(local)
@@ -275,12 +291,21 @@ def run_ours(args):
     sampler.stop()
     t_fast = max_over_ranks(t_fast, world)
     value = world * args.steps / t_fast
+    fast_launches = fast.launches
+
+    guess_val, info_guess = None, []
+    if guess_model is not None and not args.no_guess:
+        fast.guess_model = guess_model
+        t_guess, info_guess = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
+        t_guess = max_over_ranks(t_guess, world)
+        guess_val = world * args.steps / t_guess
+        fast.guess_model = None
 
     plain_val, info_plain = None, []
     if not args.no_plain:
         plain = Runner(n, "fp64", None, args.max_vcycles)
         pdev = [plain.load_device(c) for c in cases]
-        t_plain, info_plain = time_steps(plain, pdev, min(args.warmup, 1), args.steps, world, flush)
+        t_plain, info_plain = time_steps(plain, pdev, args.warmup, args.steps, world, flush)
         t_plain = max_over_ranks(t_plain, world)
         plain_val = world * args.steps / t_plain
         del plain, pdev
@@ -308,10 +333,7 @@ def run_ours(args):
         ph.set_geometry(dev["bed"], dev["H"])
         ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
         ph.reset_solution()
-        guess = None
-        if guess_model is not None:
-            guess = guess_model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"])
-        u, v, H = ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles, guess=guess)
+        u, v, H = ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles)
         out_u.copy_(u, non_blocking=True)
         out_v.copy_(v, non_blocking=True)
         b.record()
@@ -350,11 +372,14 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        cpu = cpu_baseline(cases[0], info_plain or info_fast)
+        cpu = cpu_baseline(cases[0], info_plain)
+
+    def arm(val, infos):
+        return {"value": val, "unit": "steps/s", "vcycles_per_step": [i.get("vcycles") for i in infos],
+                "finish_sweeps_per_step": [i.get("finish_sweeps") for i in infos],
+                "rel_residual_reached": [i.get("rel_residual") for i in infos]}
 
     if rank == 0:
-        vc = [i.get("vcycles") for i in info_fast]
-        rel = [i.get("rel_residual") for i in info_fast]
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_fast / args.steps, "higher_is_better": True,
@@ -362,14 +387,14 @@ def run_ours(args):
             "data": "synthetic (seeded grounded-dome geometries, fresh per step)",
             "config": {"workload": f"forward step to {TOL:g} rel. residual, {n}x{n}, dx={DX * 1024 / n:g} m, "
                                    f"{LEVELS} levels, dt={DT:g} a, fresh geometry per step",
-                       "path": "mixed" + ("+learned_guess" if guess_model is not None else ""),
+                       "path": "mixed FAS, full-step local Newton x2, FP32/FP64 finishing sweeps + Anderson(3)",
                        "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas x{world}"},
-            "vcycles_per_step": vc, "rel_residual_reached": rel,
-            "plain_fp64_fas": {"value": plain_val, "unit": "steps/s",
-                               "vcycles_per_step": [i.get("vcycles") for i in info_plain],
-                               "rel_residual_reached": [i.get("rel_residual") for i in info_plain]},
+            **{k: v for k, v in arm(value, info_fast).items() if k not in ("value", "unit")},
+            "learned_guess": (arm(guess_val, info_guess) if guess_val is not None else
+                              {"unavailable": "no trained model" if guess_model is None else "skipped"}),
+            "plain_fp64_fas": arm(plain_val, info_plain) if plain_val is not None else None,
             "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": fast.launches,
+            "gpu_launches": fast_launches,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),
@@ -424,19 +449,31 @@ def sweeps_per_vcycle(levels=LEVELS, n_smooth=10, n_local_outer=10, n_local=10, 
     return w
 
 
+def plain_step_sweeps(infos):
+    """Fine-level-equivalent sweeps of one plain FAS step: V-cycles x sweeps
+    per V-cycle + finishing sweeps, averaged over the measured steps (fixed
+    figures of an earlier GPU run of the plain arm when none are given)."""
+    vc = [i.get("vcycles") or 0 for i in infos]
+    fs = [i.get("finish_sweeps") or 0 for i in infos]
+    if not vc:
+        return REF_VCYCLES_PER_STEP, REF_FINISH_SWEEPS_PER_STEP
+    return sum(vc) / len(vc), sum(fs) / len(fs)
+
+
 def cpu_baseline(case, infos, workers=None):
     workers = workers or os.cpu_count() or 1
     t_sweep = cpu_sweep_time(case, workers)
-    vcycles = [i.get("vcycles") or 0 for i in infos] or [REF_VCYCLES_PER_STEP]
-    vpc = sum(vcycles) / len(vcycles) if vcycles else REF_VCYCLES_PER_STEP
-    t_step = vpc * sweeps_per_vcycle() * t_sweep
+    vpc, fin = plain_step_sweeps(infos)
+    t_step = (vpc * sweeps_per_vcycle() + fin) * t_sweep
     return {"value": 1.0 / t_step, "unit": "steps/s", "cores": workers, "kind": "port",
             "sample": f"one full-size {case.ny}x{case.nx} FP64 NumPy Vanka sweep ({t_sweep:.2f} s on {workers} "
-                      f"processes), scaled by {sweeps_per_vcycle():.1f} fine-equivalent sweeps per V-cycle x "
-                      f"{vpc:.1f} V-cycles per step"}
+                      f"processes), scaled by {vpc:.1f} V-cycles x {sweeps_per_vcycle():.1f} fine-equivalent "
+                      f"sweeps + {fin:.0f} finishing sweeps per step (the plain FP64 arm's counts)"}
 
 
-REF_VCYCLES_PER_STEP = 10.0
+# mean counts of the plain FP64 arm on this workload (GPU run, 3 fresh geometries)
+REF_VCYCLES_PER_STEP = 3.0
+REF_FINISH_SWEEPS_PER_STEP = 313.0
 
 
 def run_reference(args):
@@ -452,11 +489,12 @@ def run_reference(args):
         if k >= args.warmup:
             times.append(t)
     t_sweep = sum(times) / len(times)
-    t_step = REF_VCYCLES_PER_STEP * sweeps_per_vcycle() * t_sweep
+    vpc, fin = plain_step_sweeps([])
+    t_step = (vpc * sweeps_per_vcycle() + fin) * t_sweep
     value = 1.0 / t_step
     sample = (f"per step: one full-size {case.ny}x{case.nx} FP64 NumPy Vanka sweep on {workers} processes "
-              f"({t_sweep:.2f} s), scaled by {sweeps_per_vcycle():.1f} fine-equivalent sweeps per V-cycle x "
-              f"{REF_VCYCLES_PER_STEP:g} V-cycles per step")
+              f"({t_sweep:.2f} s), scaled by {vpc:g} V-cycles x {sweeps_per_vcycle():.1f} fine-equivalent sweeps "
+              f"+ {fin:g} finishing sweeps per step")
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded grounded-dome geometry)",

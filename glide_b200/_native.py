@@ -47,7 +47,10 @@ class Level(C.Structure):
                 ("chi", C.c_void_p), ("err_mask", C.c_void_p),
                 ("lam", C.c_void_p), ("f_adj", C.c_void_p), ("r_adj", C.c_void_p),
                 ("H_prev", C.c_void_p), ("smb", C.c_void_p),
-                ("scratch", C.c_void_p), ("flags", C.c_void_p), ("any_active", C.c_void_p)]
+                ("scratch", C.c_void_p), ("flags", C.c_void_p), ("any_active", C.c_void_p),
+                ("ls_tmp", C.c_void_p), ("ls_norms", C.c_void_p), ("norm_parts", C.c_void_p)]
+
+LS_CANDIDATES = 4  # GLIDE_LS_CANDIDATES
 
 
 class SolverConfig(C.Structure):
@@ -55,7 +58,7 @@ class SolverConfig(C.Structure):
                 ("n_local", C.c_int), ("n_newton", C.c_int), ("omega", C.c_double), ("shift", C.c_double),
                 ("err_threshold", C.c_double), ("adj_coarse", C.c_int), ("adj_smooth", C.c_int),
                 ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int),
-                ("newton_step", C.c_double)]
+                ("newton_step", C.c_double), ("coarse_line_search", C.c_int)]
 
 
 class NativeError(RuntimeError):

@@ -32,6 +32,8 @@ template <typename T> int launch_fill(void*, double, int64_t, cudaStream_t);
 template <typename T> int launch_mask_le(void*, const void*, const void*, double, int64_t, cudaStream_t);
 template <typename T> int launch_constraint_down(void*, void*, const void*, const void*, int, int, int, cudaStream_t);
 template <typename T> int launch_norms(double*, double*, const void*, const void*, const void*, const void*, const void*, int64_t, int64_t, int64_t, cudaStream_t);
+template <typename T> int launch_axpy_dev(void*, const void*, const double*, const void*, int64_t, cudaStream_t);
+int launch_ls_pick(double*, const double*, int, cudaStream_t);
 int norms_parts_count(int64_t n);
 
 template <typename D, typename S>
@@ -293,6 +295,31 @@ int restrict3(GlideLevel* L, GlideLevel* C, void* Vf, void* Vc, void* s) {
     return 0;
 }
 
+// U = U_pre + a * P(U_c - w_c), a from GLIDE_LS_CANDIDATES steps by the
+// smallest fine residual norm; the choice is made on the device (graph-safe).
+int line_search_correction(GlideLevel* L, GlideLevel* C, const GlideSolverConfig* c, void* s) {
+    static const double alphas[GLIDE_LS_CANDIDATES] = {1.0, 0.5, 0.25, 0.0};  // same order as ls_pick_k
+    LevelView w = view(L), wc = view(C);
+    const int64_t ntb = w.ntot * w.nb;
+    TRY(glide_prolong(w.dt, 0, 1, 0, wc.u(C->z), w.u(L->z), C->a.ny, C->a.nx, C->a.nb, s));
+    TRY(glide_prolong(w.dt, 1, 1, 0, wc.v(C->z), w.v(L->z), C->a.ny, C->a.nx, C->a.nb, s));
+    if (c->smooth_H_correction != 2)
+        TRY(glide_prolong(w.dt, 2, c->smooth_H_correction, 0, wc.H(C->z), w.H(L->z), C->a.ny, C->a.nx, C->a.nb, s));
+    else
+        TRY(glide_fill(w.dt, w.H(L->z), 0.0, w.nc * w.nb, s));
+    TRY(glide_lincomb(w.dt, L->ls_tmp, L->U, 1.0, nullptr, 0.0, ntb, s));   // U_pre
+    for (int j = 0; j < GLIDE_LS_CANDIDATES; j++) {
+        TRY(glide_lincomb(w.dt, L->U, L->ls_tmp, 1.0, L->z, alphas[j], ntb, s));
+        TRY(glide_residual(&L->a, w.u(L->f), w.v(L->f), w.H(L->f), w.u(L->r), w.v(L->r), w.H(L->r), s));
+        TRY(glide_norms(w.dt, L->ls_norms + 3 * j, L->norm_parts, w.u(L->r), w.v(L->r), w.H(L->r), L->a.H,
+                        L->a.gamma, w.nu * w.nb, w.nv * w.nb, w.nc * w.nb, s));
+    }
+    double* a_dev = L->ls_norms + 3 * GLIDE_LS_CANDIDATES;
+    TRY(launch_ls_pick(a_dev, L->ls_norms, GLIDE_LS_CANDIDATES, S(s)));
+    return (w.dt == GLIDE_F32 ? launch_axpy_dev<float> : launch_axpy_dev<double>)(L->U, L->ls_tmp, a_dev, L->z, ntb,
+                                                                                   S(s));
+}
+
 int fascd(GlideLevel* lv, int n, int k, bool finest, const GlideSolverConfig* c, void* s) {
     GlideLevel* L = &lv[k];
     LevelView w = view(L);
@@ -323,9 +350,15 @@ int fascd(GlideLevel* lv, int n, int k, bool finest, const GlideSolverConfig* c,
     TRY(fascd(lv, n, k + 1, false, c, s));
     // U += P(U_c - w_c): bilinear for u and v, injection for H   (solver.py:131-140)
     TRY(glide_lincomb(wc.dt, C->z, C->U, 1.0, C->w, -1.0, wc.ntot * wc.nb, s));
-    TRY(glide_prolong(w.dt, 0, 1, 1, wc.u(C->z), w.u(L->U), C->a.ny, C->a.nx, C->a.nb, s));
-    TRY(glide_prolong(w.dt, 1, 1, 1, wc.v(C->z), w.v(L->U), C->a.ny, C->a.nx, C->a.nb, s));
-    TRY(glide_prolong(w.dt, 2, c->smooth_H_correction, 1, wc.H(C->z), w.H(L->U), C->a.ny, C->a.nx, C->a.nb, s));
+    if (finest && c->coarse_line_search && L->ls_tmp && L->ls_norms && L->norm_parts) {
+        TRY(line_search_correction(L, C, c, s));
+    } else {
+        TRY(glide_prolong(w.dt, 0, 1, 1, wc.u(C->z), w.u(L->U), C->a.ny, C->a.nx, C->a.nb, s));
+        TRY(glide_prolong(w.dt, 1, 1, 1, wc.v(C->z), w.v(L->U), C->a.ny, C->a.nx, C->a.nb, s));
+        if (c->smooth_H_correction != 2)  // 2: velocity-only coarse correction
+            TRY(glide_prolong(w.dt, 2, c->smooth_H_correction, 1, wc.H(C->z), w.H(L->U), C->a.ny, C->a.nx,
+                              C->a.nb, s));
+    }
     // post-smoothing and local error-driven smoothing   (solver.py:143-157)
     TRY(gamma_from(L, L->chi, s));
     TRY(vanka(L, c->n_smooth, c, false, s));

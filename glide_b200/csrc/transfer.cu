@@ -189,19 +189,53 @@ __global__ void __launch_bounds__(RB) norms_partial_k(double* __restrict__ parts
         parts[3 * blockIdx.x + 2] = t2;
     }
 }
-__global__ void norms_final_k(double* __restrict__ out, const double* __restrict__ parts, int nparts) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double a = 0, b = 0, c = 0;
-        for (int k = 0; k < nparts; k++) {
-            a += parts[3 * k];
-            b += parts[3 * k + 1];
-            c += parts[3 * k + 2];
-        }
+// Sum of the per-block partials in a fixed order (thread t adds parts t, t+RB,
+// ... in sequence, then a fixed shuffle/shared-memory tree): deterministic.
+__global__ void __launch_bounds__(RB) norms_final_k(double* __restrict__ out, const double* __restrict__ parts,
+                                                     int nparts) {
+    __shared__ double sh[RB / 32];
+    double a = 0, b = 0, c = 0;
+    for (int k = threadIdx.x; k < nparts; k += RB) {
+        a += parts[3 * k];
+        b += parts[3 * k + 1];
+        c += parts[3 * k + 2];
+    }
+    a = block_sum(a, sh);
+    b = block_sum(b, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) {
         out[0] = a;
         out[1] = b;
         out[2] = c;
     }
 }
+
+// Coarse-correction line search (finest level): pick the candidate step with
+// the smallest residual norm.  norms holds 3 sums of squares per candidate.
+__global__ void ls_pick_k(double* __restrict__ alpha_out, const double* __restrict__ norms, int k) {
+    const double alphas[4] = {1.0, 0.5, 0.25, 0.0};  // GLIDE_LS_CANDIDATES, best first on ties
+    if (threadIdx.x != 0 || blockIdx.x != 0 || k < 1 || k > 4) return;
+    int best = 0;
+    double bn = norms[0] + norms[1] + norms[2];
+    for (int j = 1; j < k; j++) {
+        const double nj = norms[3 * j] + norms[3 * j + 1] + norms[3 * j + 2];
+        if (nj < bn) {  // NaN candidates never win
+            bn = nj;
+            best = j;
+        }
+    }
+    alpha_out[0] = alphas[best];
+}
+
+// out = x + alpha[0] * y with alpha read on the device.
+template <typename T>
+__global__ void axpy_dev_k(T* __restrict__ out, const T* __restrict__ x, const double* __restrict__ alpha,
+                           const T* __restrict__ y, int64_t n) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    out[k] = x[k] + T(alpha[0]) * y[k];
+}
+
 
 // --------------------------------------------------------------------------
 // launchers (batch count nb on grid.y)
@@ -275,7 +309,18 @@ int launch_norms(double* out3, double* parts, const void* r_u, const void* r_v, 
     const int nb = norms_parts_count(nu > nc ? nu : nc);
     glide::count_launch(), norms_partial_k<T><<<nb, RB, 0, s>>>(parts, (const T*)r_u, (const T*)r_v, (const T*)r_H, (const T*)H,
                                          (const T*)gamma, nu, nv, nc);
-    glide::count_launch(), norms_final_k<<<1, 32, 0, s>>>(out3, parts, nb);
+    glide::count_launch(), norms_final_k<<<1, RB, 0, s>>>(out3, parts, nb);
+    return (int)cudaGetLastError();
+}
+
+int launch_ls_pick(double* alpha_out, const double* norms, int k, cudaStream_t s) {
+    glide::count_launch(), ls_pick_k<<<1, 32, 0, s>>>(alpha_out, norms, k);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+int launch_axpy_dev(void* out, const void* x, const double* alpha, const void* y, int64_t n, cudaStream_t s) {
+    glide::count_launch(), axpy_dev_k<T><<<nblk(n), EW, 0, s>>>((T*)out, (const T*)x, alpha, (const T*)y, n);
     return (int)cudaGetLastError();
 }
 
@@ -287,7 +332,8 @@ int launch_norms(double* out3, double* parts, const void* r_u, const void* r_v, 
     template int launch_mask_le<T>(void*, const void*, const void*, double, int64_t, cudaStream_t);                \
     template int launch_constraint_down<T>(void*, void*, const void*, const void*, int, int, int, cudaStream_t);   \
     template int launch_norms<T>(double*, double*, const void*, const void*, const void*, const void*, const void*, \
-                                 int64_t, int64_t, int64_t, cudaStream_t);
+                                 int64_t, int64_t, int64_t, cudaStream_t);                                         \
+    template int launch_axpy_dev<T>(void*, const void*, const double*, const void*, int64_t, cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

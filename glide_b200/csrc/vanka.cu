@@ -465,6 +465,9 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : 1) vanka_cells_kerne
         Hc -= step * x[4];
         Hc = M<T>::max(Hc, thk);
     }
+    if (!(isfinite(ul) && isfinite(ur) && isfinite(vt) && isfinite(vb) && isfinite(Hc))) {
+        ul = ul0, ur = ur0, vt = vt0, vb = vb0, Hc = H0;  // a failed local solve leaves its cell unchanged
+    }
     const int64_t ic = int64_t(i) * nx + j;
     scratch[ic] = T(0.5) * (ul - ul0);
     scratch[nc + ic] = T(0.5) * (ur - ur0);

@@ -80,6 +80,7 @@ class Grid:
         self._flags = torch.zeros(nflags, dtype=torch.int32, device=self.device)
         self._any_active = torch.zeros(self.nb, dtype=torch.int32, device=self.device)
         self._norm_out = torch.zeros(3, dtype=torch.float64, device=self.device)
+        self._ls_tmp = self._ls_norms = None
         self._norm_parts = torch.zeros(3 * self._lib.glide_norm_parts(max(self.nu, self.nh) * self.nb),
                                        dtype=torch.float64, device=self.device)
 
@@ -110,6 +111,12 @@ class Grid:
         L.lam, L.f_adj, L.r_adj = self.Lambda.data_ptr(), self.f_adj.data_ptr(), self.r_adj.data_ptr()
         L.H_prev, L.smb = self.H_prev.data_ptr(), self.smb.data_ptr()
         L.scratch, L.flags, L.any_active = self._scratch.data_ptr(), self._flags.data_ptr(), self._any_active.data_ptr()
+        if self.parent is None:  # coarse-correction line search on the finest level only
+            if self._ls_tmp is None:
+                self._ls_tmp = self._vec()
+                self._ls_norms = torch.zeros(3 * N.LS_CANDIDATES + 1, dtype=torch.float64, device=self.device)
+            L.ls_tmp, L.ls_norms = self._ls_tmp.data_ptr(), self._ls_norms.data_ptr()
+            L.norm_parts = self._norm_parts.data_ptr()
         return L
 
     def _s(self):

@@ -272,12 +272,23 @@ class IcePhysics:
         prev = 1.0
         rel = 1.0
         stalled = False
+        good = self._good_state() if tol is not None else None
         while k < n_max:
+            if good is not None:
+                good.copy_(g.U)
             self._run_cycle()
             k += 1
             if not track:
                 continue
             rel = self.residual_norm() / r0 if r0 > 0 else 0.0
+            if good is not None and (not math.isfinite(rel) or rel > 100.0 * prev) and not (
+                    guess is not None and k == 1 and info["guess_used"]):
+                # a diverging cycle: keep the state before it and finish by relaxation
+                g.U.copy_(good)
+                info["cycle_restored"] = True
+                rel = prev
+                stalled = True
+                break
             if guess is not None and k == 1 and info["guess_used"]:
                 # judge the guess by the first cycle: it must cut |r| by guess_min_reduction
                 if not (rel * self.guess_min_reduction <= 1.0) or not math.isfinite(rel):
@@ -298,6 +309,16 @@ class IcePhysics:
             prev = rel
         if tol is not None and finish and rel > tol and (stalled or k >= n_max):
             rel = self._finish(r0, tol, max_finish_sweeps, hist, info, verbose)
+        if tol is not None and guess is not None and info["guess_used"] and not rel <= tol:
+            # the guess led somewhere the solver cannot finish from: solve again from the plain start
+            g.U.copy_(saved)
+            self.forward(dt, n_vcycles, verbose, update_geometry=False, tol=tol, max_vcycles=max_vcycles,
+                         guess=None, history=hist, finish=finish, max_finish_sweeps=max_finish_sweeps)
+            sub = self.last_info
+            k += sub["vcycles"]
+            info["finish_sweeps"] = info.get("finish_sweeps", 0) + sub["finish_sweeps"]
+            info.update(fallback=True, guess_used=False, late_fallback=True)
+            rel = sub["rel_residual"]
         info["vcycles"] = k
         info["rel_residual"] = rel if track else None
         self.last_history = hist
@@ -328,12 +349,16 @@ class IcePhysics:
         nU = g.nb * (g.nu + g.nv)
         Fs, Gs = [], []
         prev = rel
+        best, good = rel, self._good_state()
+        good.copy_(g.U)
+        since_best = 0
+        local = self._finish_local()
         while done < max_sweeps and rel > tol:
             x0 = g.U[:nU].clone() if m > 0 else None
             if use32:
-                self._fp32_sweeps(self.finish_block)
+                self._fp32_sweeps(self.finish_block, local)
             else:
-                g.vanka_sweep(self.finish_block, omega=st.omega, shift=st.shift, **self._finish_local())
+                g.vanka_sweep(self.finish_block, omega=st.omega, shift=st.shift, **local)
             done += self.finish_block
             if m > 0:
                 Gx = g.U[:nU].clone()
@@ -355,7 +380,25 @@ class IcePhysics:
             hist.append(rel)
             if verbose:
                 print(f"  finish {done} sweeps ({'fp32' if use32 else 'fp64'}): |r|/|r0| = {rel:.2e}")
-            if not math.isfinite(rel):
+            if not math.isfinite(rel) or rel > 100.0 * best:
+                # diverging relaxation: back to the best state, then the reference's damped local Newton
+                g.U.copy_(good)
+                rel = best
+                Fs, Gs = [], []
+                safe = dict(n_inner=REFERENCE.n_newton, step=REFERENCE.newton_step)
+                if local == safe:
+                    break
+                local = safe
+                info["finish_safe"] = True
+                continue
+            if rel < best:
+                if rel < 0.99 * best:
+                    since_best = 0
+                best = rel
+                good.copy_(g.U)
+            since_best += 1
+            if since_best > 10:   # no progress over 10 blocks: stop (a late guess fallback may follow)
+                info["finish_stagnated"] = True
                 break
             if use32 and rel > 0.7 * prev:
                 use32 = False           # FP32 correction floor reached: continue in FP64
@@ -371,7 +414,13 @@ class IcePhysics:
         return dict(n_inner=st.n_newton if self.finish_newton is None else self.finish_newton,
                     step=st.newton_step if self.finish_step is None else self.finish_step)
 
-    def _fp32_sweeps(self, n):
+    def _good_state(self):
+        """Preallocated copy of the state vector (the last state known to be finite)."""
+        if getattr(self, "_good", None) is None or self._good.shape != self.grid.U.shape:
+            self._good = torch.empty_like(self.grid.U)
+        return self._good
+
+    def _fp32_sweeps(self, n, local=None):
         """FP32 fine-level sweeps on the FP64 problem's correction equation."""
         g64, g32 = self.grid, self.grid32
         lib = self.kernels
@@ -386,7 +435,7 @@ class IcePhysics:
         a = g32.level_args()
         N.check(lib.glide_residual(C.byref(a), g32.r_u.data_ptr(), g32.r_v.data_ptr(), g32.r_H.data_ptr(),
                                    g32.f_u.data_ptr(), g32.f_v.data_ptr(), g32.f_H.data_ptr(), s), "residual32")
-        g32.vanka_sweep(n, omega=st.omega, shift=st.shift, **self._finish_local())
+        g32.vanka_sweep(n, omega=st.omega, shift=st.shift, **(local or self._finish_local()))
         N.check(lib.glide_lincomb(N.F32, g32.z.data_ptr(), g32.U.data_ptr(), 1.0, g32.w.data_ptr(), -1.0, ntot, s),
                 "lincomb")
         N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.z.data_ptr(), ntot, 1, s), "convert")

@@ -33,6 +33,7 @@ class SolverSettings:
     exact_adjoint: bool = False  # reference VJP/grad boundary handling when False
     smooth_H_correction: bool = False  # bilinear instead of injected coarse H correction
     newton_step: float = 0.25  # fraction of each local Newton step (relaxation_factor, glide/cuda/vanka.cu:416)
+    coarse_line_search: bool = False  # finest-level step on the coarse correction (reference: full step)
 
     def native(self, thklim) -> N.SolverConfig:
         c = N.SolverConfig()
@@ -44,6 +45,7 @@ class SolverSettings:
         c.exact_adjoint = int(self.exact_adjoint)
         c.smooth_H_correction = int(self.smooth_H_correction)
         c.newton_step = float(self.newton_step)
+        c.coarse_line_search = int(self.coarse_line_search)
         return c
 
 

@@ -155,7 +155,14 @@ typedef struct GlideLevel {
     void* scratch;          /* 5 * nc * nb */
     int* flags;             /* (ny/14+1) * (nx/14+1) * nb */
     int* any_active;        /* nb */
+    /* coarse-correction line search (finest level; may be null when off) */
+    void* ls_tmp;           /* one state vector (like U) */
+    double* ls_norms;       /* 3 * GLIDE_LS_CANDIDATES + 1 doubles */
+    double* norm_parts;     /* 3 * glide_norm_parts(max(nu, nc) * nb) doubles */
 } GlideLevel;
+
+/* Step sizes tried by the coarse-correction line search, best first on ties. */
+#define GLIDE_LS_CANDIDATES 4
 
 typedef struct GlideSolverConfig {
     double thklim;
@@ -164,9 +171,13 @@ typedef struct GlideSolverConfig {
     int adj_coarse, adj_smooth;
     double adj_omega;
     int exact_adjoint;      /* 0: reference VJP boundary handling */
-    int smooth_H_correction;/* 0: inject the coarse H correction (reference), 1: bilinear */
+    int smooth_H_correction;/* 0: inject the coarse H correction (reference), 1: bilinear,
+                               2: no H correction (velocity-only coarse correction) */
     double newton_step;     /* fraction of each local Newton step taken in the forward sweeps;
                                <= 0 means the reference's GLIDE_REF_NEWTON_STEP */
+    int coarse_line_search; /* 1: on the finest level, U = U_pre + a * P(U_c - w_c) with a in
+                               {1, 1/2, 1/4, 0} minimising the residual norm (chosen on the
+                               device); 0: a = 1 (reference) */
 } GlideSolverConfig;
 
 /* One FASCD V-cycle from level k0 (finest=1 sets w=U, chi=gamma-H first). */

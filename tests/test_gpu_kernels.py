@@ -251,3 +251,24 @@ def test_batch_matches_single():
         g1 = _grid(st, "fp64")
         g1.compute_residual()
         assert torch.equal(g.r_u[b], g1.r_u) and torch.equal(g.r_v[b], g1.r_v) and torch.equal(g.r_H[b], g1.r_H)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vanka_failed_local_solve_leaves_cell_unchanged(precision):
+    """A non-finite right-hand side at one face makes the two cells sharing it
+    fail their local solve: those cells keep their values, every other update
+    matches the sweep without the bad value, and nothing turns non-finite."""
+    st = _state((24, 40), seed=7)
+    st["u"] *= 0.02
+    st["v"] *= 0.02
+    good, bad = _grid(st, precision), _grid(st, precision)
+    i, j = 10, 17
+    bad.f_u[i, j] = float("nan")
+    for g in (good, bad):
+        g.vanka_sweep(1, n_inner=2, omega=0.5, shift=0.0, step=1.0)
+    assert torch.isfinite(bad.U).all()
+    assert bad.H[i, j - 1] == torch.as_tensor(st["H"][i, j - 1], dtype=bad.dtype)
+    assert bad.H[i, j] == torch.as_tensor(st["H"][i, j], dtype=bad.dtype)
+    far = torch.ones_like(bad.H, dtype=torch.bool)
+    far[max(i - 2, 0):i + 3, max(j - 3, 0):j + 3] = False
+    assert torch.equal(bad.H[far], good.H[far])
