@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--max-vcycles", type=int, default=40)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 FAS comparison arm")
     ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess arm")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--no-clocks", action="store_true", help="do not sample nvidia-smi clocks")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch kernels one by one instead of replaying CUDA graphs (for profiler runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     return ap.parse_args()
 
@@ -268,51 +272,11 @@ def dominant_kernel_timing(runner, sweeps=20):
     return t_vanka, t_res, g
 
 
-def run_ours(args):
-    import torch
-    world, rank, local = dist_setup(args)
-    n = args.n
-    seeds = [rank * 100_000 + k for k in range(args.warmup + args.steps)]
-    cases = make_cases(n, seeds)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
-
-    guess_model = None
-    try:
-        from glide_b200.guess import load_default_model
-        guess_model = load_default_model()
-    except Exception as e:  # the learned-guess arm is reported as unavailable
-        print(f"learned guess unavailable: {e}", file=sys.stderr)
-    fast = Runner(n, "mixed", None, args.max_vcycles, fast_settings(), **FAST_KW)
-    fdev = [fast.load_device(c) for c in cases]
-
-    sampler = ClockSampler(local)
-    sampler.start()
-    t_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
-    sampler.stop()
-    t_fast = max_over_ranks(t_fast, world)
-    value = world * args.steps / t_fast
-    fast_launches = fast.launches
-
-    guess_val, info_guess = None, []
-    if guess_model is not None and not args.no_guess:
-        fast.guess_model = guess_model
-        t_guess, info_guess = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
-        t_guess = max_over_ranks(t_guess, world)
-        guess_val = world * args.steps / t_guess
-        fast.guess_model = None
-
-    plain_val, info_plain = None, []
-    if not args.no_plain:
-        plain = Runner(n, "fp64", None, args.max_vcycles)
-        pdev = [plain.load_device(c) for c in cases]
-        t_plain, info_plain = time_steps(plain, pdev, args.warmup, args.steps, world, flush)
-        t_plain = max_over_ranks(t_plain, world)
-        plain_val = world * args.steps / t_plain
-        del plain, pdev
-
-    # end to end through the public API: host (pinned) inputs, H2D each step, D2H of u, v
+def end_to_end(fast, cases, args, world, flush, n):
+    """Steps/s through IcePhysics with host (pinned) inputs: every step copies
+    its inputs host->device and reads (u, v) back inside the timed region."""
     import numpy as np
-    e2e_val, h2d, d2h = None, 0, 0
+    import torch
     host = []
     for c in cases:
         d = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float64).pin_memory()
@@ -343,7 +307,54 @@ def run_ours(args):
     h2d = sum(t.numel() * t.element_size() for t in host[0].values())
     d2h = out_u.numel() * 8 + out_v.numel() * 8
     tot = max_over_ranks(tot, world)
-    e2e_val = world * args.steps / tot
+    return world * args.steps / tot, h2d, d2h
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    n = args.n
+    seeds = [rank * 100_000 + k for k in range(args.warmup + args.steps)]
+    cases = make_cases(n, seeds)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    guess_model = None
+    try:
+        from glide_b200.guess import load_default_model
+        guess_model = load_default_model()
+    except Exception as e:  # the learned-guess arm is reported as unavailable
+        print(f"learned guess unavailable: {e}", file=sys.stderr)
+    fast = Runner(n, "mixed", None, args.max_vcycles, fast_settings(), use_graphs=not args.eager, **FAST_KW)
+    fdev = [fast.load_device(c) for c in cases]
+
+    sampler = ClockSampler(local)
+    if not args.no_clocks:
+        sampler.start()
+    t_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
+    sampler.stop()
+    t_fast = max_over_ranks(t_fast, world)
+    value = world * args.steps / t_fast
+    fast_launches = fast.launches
+
+    guess_val, info_guess = None, []
+    if guess_model is not None and not args.no_guess:
+        fast.guess_model = guess_model
+        t_guess, info_guess = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
+        t_guess = max_over_ranks(t_guess, world)
+        guess_val = world * args.steps / t_guess
+        fast.guess_model = None
+
+    plain_val, info_plain = None, []
+    if not args.no_plain:
+        plain = Runner(n, "fp64", None, args.max_vcycles, use_graphs=not args.eager)
+        pdev = [plain.load_device(c) for c in cases]
+        t_plain, info_plain = time_steps(plain, pdev, args.warmup, args.steps, world, flush)
+        t_plain = max_over_ranks(t_plain, world)
+        plain_val = world * args.steps / t_plain
+        del plain, pdev
+
+    # end to end through the public API: host (pinned) inputs, H2D each step, D2H of u, v
+    e2e_val, h2d, d2h = (None, 0, 0) if args.no_e2e else end_to_end(fast, cases, args, world, flush, n)
 
     # dominant-kernel roofline (Vanka cell kernel, fine level of the FP32 hierarchy)
     t_vanka, t_res, g = dominant_kernel_timing(fast)

@@ -23,9 +23,20 @@ long long launch_total();
 // precision helpers
 // --------------------------------------------------------------------------
 template <typename T> struct M;
+// FP32 exp/pow: the hardware approximations by default, as the reference's
+// --use_fast_math build of its ice kernels uses (glide/kernels.py:72);
+// -DGLIDE_FP32_ACCURATE_MATH=1 selects expf/powf.
+#ifndef GLIDE_FP32_ACCURATE_MATH
+#define GLIDE_FP32_ACCURATE_MATH 0
+#endif
 template <> struct M<float> {
+#if GLIDE_FP32_ACCURATE_MATH
     static __device__ __forceinline__ float exp(float x) { return expf(x); }
     static __device__ __forceinline__ float pow(float x, float y) { return powf(x, y); }
+#else
+    static __device__ __forceinline__ float exp(float x) { return __expf(x); }
+    static __device__ __forceinline__ float pow(float x, float y) { return __powf(x, y); }
+#endif
     static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float abs(float x) { return fabsf(x); }
     static __device__ __forceinline__ float copysign(float a, float b) { return copysignf(a, b); }

@@ -416,7 +416,10 @@ template <typename T> __device__ __forceinline__ void lu5_solve_fast(T (&A)[25],
 // Per-cell Newton deltas.  scratch holds 5 cell arrays: 0.5*du_l, 0.5*du_r,
 // 0.5*dv_t, 0.5*dv_b, dH.
 template <typename T, bool LOCAL>
-__global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : 1) vanka_cells_kernel(
+#ifndef GLIDE_VANKA64_MIN_BLOCKS
+#define GLIDE_VANKA64_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BLOCKS) vanka_cells_kernel(
     T* __restrict__ scratch, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, const T* __restrict__ bed,
     const T* __restrict__ B, const T* __restrict__ beta, const T* __restrict__ gamma, const int* __restrict__ flags,
