@@ -16,7 +16,9 @@ Arms
                      finishing sweeps with Anderson acceleration.  Beside it:
                      the same path started from the learned initial guess
                      (``learned_guess``), and the plain FP64 FAS path with the
-                     reference's smoother (``plain_fp64_fas``).
+                     reference's smoother (``plain_fp64_fas``), and both paths
+                     on a time series started from the previous step's
+                     solution (``warm_start``; the reference steps this way).
   --impl reference   the plain FAS algorithm in FP64 NumPy on the host cores
                      (the reference itself is GPU-only), timed on a bounded
                      sample: full-size fine-level Vanka sweeps, scaled to a
@@ -57,6 +59,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 FAS comparison arm")
     ap.add_argument("--no-guess", action="store_true", help="skip the learned-guess arm")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--no-warm", action="store_true", help="skip the warm-start (time series) variant")
     ap.add_argument("--no-clocks", action="store_true", help="do not sample nvidia-smi clocks")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying CUDA graphs (for profiler runs)")
@@ -240,36 +243,109 @@ def time_steps(runner, devs, warmup, steps, world, flush):
     return total, infos
 
 
-def dominant_kernel_timing(runner, sweeps=20):
-    """Average duration of the fine-level Vanka cell kernel (CUDA events on the
-    launching stream) and of the residual kernel on the solved state."""
+def kernel_timings(runner, launches=20):
+    """Average launch durations (CUDA events on the launching stream) on the
+    solved 1024^2 state of the fast path: the fine-level Vanka cell kernel in
+    FP64 (the finishing sweeps) and FP32 (the V-cycle smoothing), with the
+    fast path's local Newton settings, and the residual stencil in both."""
     import ctypes as C
     import torch
     from glide_b200 import _native as N
     ph = runner.ph
-    g = ph._solve_grids[0]
     lib = N.load()
     s = torch.cuda.current_stream()
-    a = g.level_args()
-    # cells kernel alone: glide_vanka_cells (no apply) through the sweep entry with omega=0 is not
-    # separable, so time sweeps and apply-only passes and subtract
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    saved = g.U.clone()
-    torch.cuda.synchronize()
-    ev[0].record(s)
-    N.check(lib.glide_vanka_cells(C.byref(a), g.f_u.data_ptr(), g.f_v.data_ptr(), g.f_H.data_ptr(), sweeps,
-                                  ph.settings.n_newton,
-                                  float(ph.settings.shift), None, None, g._scratch.data_ptr(), s.cuda_stream),
-            "vanka cells")
-    ev[1].record(s)
-    for _ in range(sweeps):
-        g.compute_residual()
-    ev[2].record(s)
-    torch.cuda.synchronize()
-    g.U.copy_(saved)
-    t_vanka = ev[0].elapsed_time(ev[1]) / 1e3 / sweeps
-    t_res = ev[1].elapsed_time(ev[2]) / 1e3 / sweeps
-    return t_vanka, t_res, g
+    n_newton = ph.finish_newton if ph.finish_newton is not None else ph.settings.n_newton
+    out = {}
+    for g, tag in ((ph.grid, "64"), (ph.grid32, "32")):
+        if g is None:
+            continue
+        a = g.level_args()
+        saved = g.r.clone()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        for rep in range(2):  # first pass warms up
+            torch.cuda.synchronize()
+            ev[0].record(s)
+            N.check(lib.glide_vanka_cells(C.byref(a), g.f_u.data_ptr(), g.f_v.data_ptr(), g.f_H.data_ptr(), launches,
+                                          n_newton, float(ph.settings.shift), None, None, g._scratch.data_ptr(),
+                                          s.cuda_stream), "vanka cells")
+            ev[1].record(s)
+            for _ in range(launches):
+                g.compute_residual()
+            ev[2].record(s)
+            torch.cuda.synchronize()
+        g.r.copy_(saved)
+        out["cells" + tag] = ev[0].elapsed_time(ev[1]) / 1e3 / launches
+        out["resid" + tag] = ev[1].elapsed_time(ev[2]) / 1e3 / launches
+    return out
+
+
+def roofline(t, n):
+    """Roofline object of the dominant kernel (the FP64 Vanka cell kernel of
+    the finishing sweeps) plus the FP32 cell kernel and the residual stencils."""
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    ncell = n * n
+    scale = ncell / (1024 * 1024)
+    def hbm_obj(bytes_per_cell, esz, sec):
+        b = ncell * bytes_per_cell * esz
+        return b / sec / 1e9
+    fp64_peak = 148 * 64 * 2 * 1.965e9 / 1e12    # DFMA 64/clk/SM (ncu), nominal clock
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    t64, t32 = t["cells64"], t.get("cells32")
+    ach = hbm_obj(VANKA_ARRAYS, 8, t64)
+    roof = {"bound": "hbm", "kernel": "vanka_cells_kernel<double> (fine level, finishing sweeps)",
+            "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "peak_source": src,
+            "traffic": VANKA64_DRAM_BYTES_1024 * scale, "traffic_source": "ncu dram__bytes_read+write, one 1024^2 launch",
+            "algorithmic_bytes": ncell * VANKA_ARRAYS * 8, "launch_ms": t64 * 1e3,
+            "limiter": "FP64 issue/latency (ncu: FP64 pipe 33%, 8 warps/SM at 214 registers before the 2-blocks/SM build)",
+            "alu": {"achieved_tflops": ncell * VANKA64_FLOPS_PER_CELL / t64 / 1e12, "peak_tflops": fp64_peak,
+                    "frac": ncell * VANKA64_FLOPS_PER_CELL / t64 / 1e12 / fp64_peak,
+                    "flops_per_cell": VANKA64_FLOPS_PER_CELL, "peak_source": "nominal FP64 (148 SMs x 64 DFMA/clk)"}}
+    if t32:
+        roof["fp32_cells"] = {"kernel": "vanka_cells_kernel<float> (fine level)", "launch_ms": t32 * 1e3,
+                              "achieved_tflops": ncell * VANKA32_FLOPS_PER_CELL / t32 / 1e12,
+                              "frac_fp32_peak": ncell * VANKA32_FLOPS_PER_CELL / t32 / 1e12 / fp32_peak,
+                              "hbm_frac": hbm_obj(VANKA_ARRAYS, 4, t32) / hbm}
+    roof["stencil"] = {k: {"launch_ms": t[k] * 1e3, "achieved": hbm_obj(RESID_ARRAYS, e, t[k]),
+                           "frac": hbm_obj(RESID_ARRAYS, e, t[k]) / hbm}
+                       for k, e in (("resid64", 8), ("resid32", 4)) if k in t}
+    return roof
+
+
+def warm_start(runner, case, args, world, flush):
+    """Steps/s of a time series on one geometry, each step started from the
+    previous step's solution (the reference's way of stepping): W untimed and
+    K timed consecutive steps, H_prev updated after each."""
+    import torch
+    ph = runner.ph
+    dev = runner.load_device(case)
+    ph.set_geometry(dev["bed"], dev["H"])
+    ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
+    ph.reset_solution()
+    tot, infos = 0.0, []
+    for k in range(args.warmup + args.steps):
+        flush_l2(flush)
+        barrier(world)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles)
+        b.record()
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            tot += a.elapsed_time(b) / 1e3
+            infos.append(dict(ph.last_info))
+    tot = max_over_ranks(tot, world)
+    return {"value": world * args.steps / tot, "unit": "steps/s",
+            "vcycles_per_step": [i.get("vcycles") for i in infos],
+            "finish_sweeps_per_step": [i.get("finish_sweeps") for i in infos],
+            "rel_residual_reached": [i.get("rel_residual") for i in infos],
+            "series": f"steps {args.warmup + 1}..{args.warmup + args.steps} of one geometry, dt={DT:g} a"}
 
 
 def end_to_end(fast, cases, args, world, flush, n):
@@ -357,29 +433,15 @@ def run_ours(args):
     e2e_val, h2d, d2h = (None, 0, 0) if args.no_e2e else end_to_end(fast, cases, args, world, flush, n)
 
     # dominant-kernel roofline (Vanka cell kernel, fine level of the FP32 hierarchy)
-    t_vanka, t_res, g = dominant_kernel_timing(fast)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    esz = 4
-    ncell = n * n
-    vanka_bytes = ncell * esz * (10 + 5)          # 10 arrays read, 5 per-cell delta arrays written
-    res_bytes = ncell * esz * 14                  # 11 read + 3 written (u/v faces ~ cells)
-    vanka_flops = ncell * VANKA_FLOPS_PER_CELL_F32
-    fp32_peak_tf = 148 * 128 * 2 * 1.965e9 / 1e12
-    roof = {"bound": "hbm", "kernel": "vanka_cells_kernel<float> (fine level)", "achieved": vanka_bytes / t_vanka / 1e9,
-            "peak": hbm_peak, "unit": "GB/s", "frac": vanka_bytes / t_vanka / 1e9 / hbm_peak,
-            "traffic": VANKA_TRAFFIC_BYTES_PER_CELL_F32 * ncell if VANKA_TRAFFIC_BYTES_PER_CELL_F32 else None,
-            "peak_source": peak_src, "launch_ms": t_vanka * 1e3,
-            "alu": {"achieved_tflops": vanka_flops / t_vanka / 1e12, "peak_tflops": fp32_peak_tf,
-                    "frac": vanka_flops / t_vanka / 1e12 / fp32_peak_tf, "peak_source": "nominal FP32 (no measured peak)",
-                    "flops_per_cell": VANKA_FLOPS_PER_CELL_F32},
-            "stencil": {"kernel": "stencil_kernel<float,false> residual", "achieved": res_bytes / t_res / 1e9,
-                        "frac": res_bytes / t_res / 1e9 / hbm_peak, "launch_ms": t_res * 1e3}}
+    roof = roofline(kernel_timings(fast), n)
+
+    warm = None
+    if not args.no_warm:
+        warm = {"fast": warm_start(fast, cases[0], args, world, flush)}
+        if not args.no_plain:
+            plain_w = Runner(n, "fp64", None, args.max_vcycles, use_graphs=not args.eager)
+            warm["plain_fp64_fas"] = warm_start(plain_w, cases[0], args, world, flush)
+            del plain_w
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -404,6 +466,7 @@ def run_ours(args):
             "learned_guess": (arm(guess_val, info_guess) if guess_val is not None else
                               {"unavailable": "no trained model" if guess_model is None else "skipped"}),
             "plain_fp64_fas": arm(plain_val, info_plain) if plain_val is not None else None,
+            "warm_start": warm,
             "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": fast_launches,
             "roofline": roof,
@@ -416,10 +479,16 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-# per-cell figures of the FP32 Vanka cell kernel (10 Newton iterations),
-# from the ncu instruction counts of one fine-level launch
-VANKA_FLOPS_PER_CELL_F32 = 6000.0
-VANKA_TRAFFIC_BYTES_PER_CELL_F32 = None
+# Per-cell figures of the fine-level Vanka cell kernel with 2 local Newton
+# iterations, from ncu op counts of one 1024^2 launch (dadd + dmul + 2 dfma,
+# fadd + fmul + 2 ffma per cell), and its DRAM bytes per launch.
+VANKA64_FLOPS_PER_CELL = 1611.0
+VANKA32_FLOPS_PER_CELL = 1324.0
+VANKA64_DRAM_BYTES_1024 = 100.46e6
+# algorithmic arrays per cell: Vanka reads u, v, H, f_u, f_v, f_H, bed, B,
+# beta, gamma and writes 5 delta arrays; the residual reads 11 and writes 3
+VANKA_ARRAYS = 15
+RESID_ARRAYS = 14
 
 
 # ---------------------------------------------------------------------------
