@@ -1,0 +1,166 @@
+"""Multi-resolution inversion of basal friction on the adjoint path.
+
+Restates the coarse-to-fine driver of examples/antarctica/antarctica_inverse.py:
+148-289 on this package: observations are restricted to every multigrid level
+(:128-138); from the coarsest level to the finest, L-BFGS-B (scipy's
+``fmin_l_bfgs_b``, bounds (-6, 5) on log(beta), ``factr`` 1e10, ``m`` 15)
+minimises misfit + ``reg_weight`` * Tikhonov(beta) over log(beta); the optimum
+is prolongated (bilinear, glide/kernels.py:216-236) as the next level's start.
+
+One objective evaluation at level k (antarctica_inverse.py:174-241):
+beta = exp(x); u = v = 0, H = H_prev; restrict the parameters below k;
+f_H = H_prev/dt + smb; forward V-cycles on the sub-hierarchy from k; misfit and
+its gradient; f_adj = -dL/d(u, v), Lambda = 0; adjoint V-cycles; grad_beta;
+d/d(log beta) = beta * grad_beta; plus the regulariser.
+
+Two switches go beyond the reference:
+
+* ``tol`` / ``adj_tol`` on the finest level solve forward and adjoint to a
+  relative residual with ``IcePhysics.forward``/``adjoint`` (the reference runs
+  5 forward and 2 adjoint V-cycles, so its gradient is the adjoint of an
+  unconverged state);
+* ``consistent_reg``: the reference adds the Tikhonov gradient taken with
+  respect to beta to the gradient with respect to log(beta)
+  (antarctica_inverse.py:230-235); with ``consistent_reg=True`` it is
+  multiplied by beta first (the chain rule), so that the objective and its
+  gradient agree.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from .kernels import prolongate_cell_centered, restrict_hfacet, restrict_vfacet
+from .physics import abs_grad, abs_loss, huber_grad, huber_loss, tikhonov_regularization
+from .solver import adjoint_vcycle, fascd_vcycle, restrict_parameters_to_hierarchy
+
+LOSSES = {"abs": (abs_loss, abs_grad), "huber": (huber_loss, huber_grad)}
+
+
+def observation_hierarchy(physics, u_obs, v_obs):
+    """(u_obs, v_obs) on every level, finest first (antarctica_inverse.py:128-133)."""
+    g = physics.grid
+    u = torch.as_tensor(u_obs, dtype=g.dtype, device=g.device)
+    v = torch.as_tensor(v_obs, dtype=g.dtype, device=g.device)
+    out = [(u, v)]
+    while g.child is not None:
+        u, v = restrict_vfacet(u), restrict_hfacet(v)
+        out.append((u, v))
+        g = g.child
+    return out
+
+
+class LevelObjective:
+    """Misfit + regulariser and its gradient in log(beta) at one level."""
+
+    def __init__(self, physics, level, u_obs, v_obs, dt, *, reg_weight=1e-4, loss="abs", n_vcycles=5,
+                 n_adjoint_vcycles=2, tol=None, adj_tol=None, exact=False, consistent_reg=False):
+        if physics.precision == "mixed":
+            raise ValueError("the inversion runs on the fp32 or fp64 hierarchy")
+        self.ph = physics
+        self.level = int(level)
+        self.grid = physics.grids[self.level]
+        self.u_obs, self.v_obs = u_obs, v_obs
+        self.dt = float(dt)
+        self.reg_weight = float(reg_weight)
+        self.loss, self.loss_grad = LOSSES[loss]
+        self.n_vcycles, self.n_adjoint = int(n_vcycles), int(n_adjoint_vcycles)
+        self.tol, self.adj_tol, self.exact = tol, adj_tol, bool(exact)
+        self.consistent_reg = bool(consistent_reg)
+        self.evaluations = 0
+        self.last = {}
+
+    def _forward(self, g):
+        ph = self.ph
+        if self.level == 0 and self.tol is not None:
+            ph.reset_solution()
+            ph.forward(self.dt, tol=self.tol, update_geometry=False)
+            return
+        g.u.zero_()
+        g.v.zero_()
+        g.H.copy_(g.H_prev)
+        restrict_parameters_to_hierarchy(g)
+        g.f_H.copy_(g.H_prev / g.dt + g.smb)
+        for _ in range(self.n_vcycles):
+            fascd_vcycle(g, ph.thklim, finest=True, settings=ph.settings)
+
+    def _adjoint(self, g, du, dv):
+        ph = self.ph
+        if self.level == 0 and self.adj_tol is not None:
+            return ph.adjoint(du, dv, torch.zeros_like(g.H), tol=self.adj_tol, exact=self.exact)
+        g.f_adj_u.copy_(-du)
+        g.f_adj_v.copy_(-dv)
+        g.f_adj_H.zero_()
+        g.Lambda.zero_()
+        saved = ph.settings.exact_adjoint
+        ph.settings.exact_adjoint = self.exact
+        try:
+            for _ in range(self.n_adjoint):
+                adjoint_vcycle(g, ph.settings, ph.thklim)
+        finally:
+            ph.settings.exact_adjoint = saved
+        return g.compute_grad_beta(exact_boundary=self.exact)
+
+    def __call__(self, x):
+        """(objective, gradient) for L-BFGS-B; x = log(beta) as float64, flattened."""
+        g = self.grid
+        for lv in self.ph.grids[self.level:]:
+            lv.dt = self.dt
+        self.ph._set_dt(self.dt)
+        log_beta = torch.as_tensor(np.asarray(x, dtype=np.float64).reshape(g.ny, g.nx), device=g.device)
+        g.beta.copy_(torch.exp(log_beta).to(g.dtype))
+        self._forward(g)
+        J = float(self.loss(g.u, g.v, self.u_obs, self.v_obs))
+        du, dv = self.loss_grad(g.u, g.v, self.u_obs, self.v_obs)
+        grad_beta = self._adjoint(g, du.to(g.dtype), dv.to(g.dtype))
+        grad = g.beta * grad_beta
+        tik, tik_grad = tikhonov_regularization(g.beta)
+        if self.consistent_reg:
+            tik_grad = tik_grad * g.beta
+        total = J + self.reg_weight * tik
+        grad = grad + self.reg_weight * tik_grad
+        self.evaluations += 1
+        self.last = {"misfit": J, "reg": self.reg_weight * tik, "total": total}
+        return total, grad.double().cpu().numpy().ravel()
+
+
+def invert_beta(physics, u_obs, v_obs, dt, *, reg_weight=1e-4, loss="abs", bounds=(-6.0, 5.0), factr=1e10, m=15,
+                maxiter=15000, levels=None, n_vcycles=5, n_adjoint_vcycles=2, tol=None, adj_tol=None, exact=False,
+                consistent_reg=False, callback=None):
+    """Coarse-to-fine L-BFGS-B over log(beta) (antarctica_inverse.py:148-289).
+
+    ``physics`` carries the geometry, B, smb and the starting beta.  ``levels``
+    lists the level indices to optimise, coarsest first (default: all).
+    Returns the finest optimised beta (a tensor, also left in physics.grid.beta)
+    and one record per level (objective evaluations, final misfit, scipy info).
+    """
+    from scipy.optimize import fmin_l_bfgs_b
+
+    obs = observation_hierarchy(physics, u_obs, v_obs)
+    grids = physics.grids
+    order = list(range(len(grids) - 1, -1, -1)) if levels is None else list(levels)
+    # the starting beta of the coarsest optimised level comes from the finest one
+    restrict_parameters_to_hierarchy(physics.grid)
+    records = []
+    for pos, k in enumerate(order):
+        g = grids[k]
+        obj = LevelObjective(physics, k, obs[k][0], obs[k][1], dt, reg_weight=reg_weight, loss=loss,
+                             n_vcycles=n_vcycles, n_adjoint_vcycles=n_adjoint_vcycles,
+                             tol=tol if k == 0 else None, adj_tol=adj_tol if k == 0 else None, exact=exact,
+                             consistent_reg=consistent_reg)
+        x0 = torch.log(g.beta).double().cpu().numpy().ravel()
+        f0, _ = obj(x0)
+        first = dict(obj.last)
+        cb = (lambda xk, _k=k: callback(_k, xk)) if callback is not None else None
+        x, f, info = fmin_l_bfgs_b(obj, x0, bounds=[bounds] * x0.size, factr=factr, m=m, maxiter=maxiter,
+                                   callback=cb)
+        g.beta.copy_(torch.exp(torch.as_tensor(x.reshape(g.ny, g.nx), device=g.device)).to(g.dtype))
+        g.mask.zero_()
+        records.append({"level": k, "shape": (g.ny, g.nx), "evaluations": obj.evaluations, "initial": first,
+                        "final_total": float(f), "final_misfit": obj.last.get("misfit", math.nan),
+                        "warnflag": int(info["warnflag"]), "iterations": int(info["nit"])})
+        if pos + 1 < len(order) and order[pos + 1] == k - 1:
+            prolongate_cell_centered(g.beta, H_fine=grids[k - 1].beta)
+    return physics.grid.beta, records
