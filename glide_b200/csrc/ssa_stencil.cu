@@ -231,6 +231,165 @@ __global__ void __launch_bounds__(NTHR) stencil_kernel(
     }
 }
 
+// --------------------------------------------------------------------------
+// residual r = F(U) - f with every input read once (glide/cuda/residuals.cu:
+// 6-292).  Same tile, phases and arithmetic as stencil_kernel<T,false>, but u,
+// v, H, bed and beta of the tile plus the rings the stencil needs are staged
+// into shared memory first with coalesced row loads; the clamped-index rule
+// is applied once while staging (a staged entry at global (i, j) holds the
+// value of the clamped index), so every later read is a plain shared-memory
+// read at unclamped global coordinates.
+// --------------------------------------------------------------------------
+constexpr int RU_R = TY + 4, RU_C = TX + 3;   // u rows [i0-2, i0+TY+2), cols [j0-1, j0+TX+2)
+constexpr int RV_R = TY + 3, RV_C = TX + 4;   // v rows [i0-1, i0+TY+2), cols [j0-2, j0+TX+2)
+constexpr int RC_R = TY + 2, RC_C = TX + 2;   // cells rows [i0-1, i0+TY+1), cols [j0-1, j0+TX+1)
+
+#ifndef GLIDE_RES_MINB32
+#define GLIDE_RES_MINB32 4
+#endif
+#ifndef GLIDE_RES_MINB64
+#define GLIDE_RES_MINB64 3
+#endif
+template <typename T>
+__global__ void __launch_bounds__(NTHR, sizeof(T) == 4 ? GLIDE_RES_MINB32 : GLIDE_RES_MINB64) residual_kernel(
+    T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
+    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
+    const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H,
+    const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
+    const T* __restrict__ mask, const T* __restrict__ gamma, Geo g, Phys<T> p) {
+    __shared__ T s_u[RU_R][RU_C];
+    __shared__ T s_v[RV_R][RV_C];
+    __shared__ T s_H[RC_R][RC_C];
+    __shared__ T s_bed[RC_R][RC_C];
+    __shared__ T s_beta[RC_R][RC_C];
+    __shared__ T s_etaH[WR][WC];
+    __shared__ T s_sxx[TY][WC];           // cells rows [i0,i0+TY), cols [j0-1, j0+TX+1)
+    __shared__ T s_syy[WR][TX];           // cells rows [i0-1,i0+TY+1), cols [j0, j0+TX)
+    __shared__ T s_sxy[TY + 1][TX + 1];   // vertices rows [i0, i0+TY], cols [j0, j0+TX]
+
+    const int ny = g.ny, nx = g.nx;
+    const int b = blockIdx.z;
+    u += b * g.nu(); v += b * g.nv(); H += b * g.nc();
+    f_u += b * g.nu(); f_v += b * g.nv(); f_H += b * g.nc();
+    bed += b * g.nc(); B += b * g.nc(); beta += b * g.nc(); mask += b * g.nc(); gamma += b * g.nc();
+    o_u += b * g.nu(); o_v += b * g.nv(); o_H += b * g.nc();
+    const TileIdx t = tile_idx<TY>();
+    const T dxi = p.dxi;
+    const int ur0 = t.i0 - 2, uc0 = t.j0 - 1, vr0 = t.i0 - 1, vc0 = t.j0 - 2, cr0 = t.i0 - 1, cc0 = t.j0 - 1;
+
+    stage(&s_u[0][0], u, ny, nx + 1, ur0, uc0, RU_R, RU_C, t.tid, NTHR);
+    stage(&s_v[0][0], v, ny + 1, nx, vr0, vc0, RV_R, RV_C, t.tid, NTHR);
+    stage(&s_H[0][0], H, ny, nx, cr0, cc0, RC_R, RC_C, t.tid, NTHR);
+    stage(&s_bed[0][0], bed, ny, nx, cr0, cc0, RC_R, RC_C, t.tid, NTHR);
+    stage(&s_beta[0][0], beta, ny, nx, cr0, cc0, RC_R, RC_C, t.tid, NTHR);
+    __syncthreads();
+    auto U = [&](int i, int j) -> T { return s_u[i - ur0][j - uc0]; };
+    auto V = [&](int i, int j) -> T { return s_v[i - vr0][j - vc0]; };
+
+    // phase 1: eta*H on the window (cells clamped into the domain)
+    for (int k = t.tid; k < WR * WC; k += NTHR) {
+        int r = k / WC, c = k - r * WC;
+        int ic = clampi(t.i0 - 1 + r, 0, ny - 1), jc = clampi(t.j0 - 1 + c, 0, nx - 1);
+        EtaIn<T> a;
+        a.ul = U(ic, jc);          a.ur = U(ic, jc + 1);
+        a.vt = V(ic, jc);          a.vb = V(ic + 1, jc);
+        a.u_tl = U(ic - 1, jc);    a.u_tr = U(ic - 1, jc + 1);
+        a.u_bl = U(ic + 1, jc);    a.u_br = U(ic + 1, jc + 1);
+        a.v_lt = V(ic, jc - 1);    a.v_rt = V(ic, jc + 1);
+        a.v_lb = V(ic + 1, jc - 1); a.v_rb = V(ic + 1, jc + 1);
+        EtaOut<T> e = cell_eta(a, __ldg(B + int64_t(ic) * nx + jc), ic, jc, ny, nx, p);
+        s_etaH[r][c] = e.eta * s_H[ic - cr0][jc - cc0];
+    }
+    __syncthreads();
+
+    // phase 2: normal stresses on cells, shear stresses on vertices
+    for (int k = t.tid; k < TY * WC; k += NTHR) {
+        int r = k / WC, c = k - r * WC;
+        int i = t.i0 + r, j = t.j0 - 1 + c;
+        s_sxx[r][c] = normal_stress<T, true>(U(i, j), U(i, j + 1), V(i, j), V(i + 1, j), s_etaH[r + 1][c], dxi,
+                                             j >= 0 && j < nx).res;
+    }
+    for (int k = t.tid; k < WR * TX; k += NTHR) {
+        int r = k / TX, c = k - r * TX;
+        int i = t.i0 - 1 + r, j = t.j0 + c;
+        s_syy[r][c] = normal_stress<T, false>(U(i, j), U(i, j + 1), V(i, j), V(i + 1, j), s_etaH[r][c + 1], dxi,
+                                              i >= 0 && i < ny).res;
+    }
+    for (int k = t.tid; k < (TY + 1) * (TX + 1); k += NTHR) {
+        int r = k / (TX + 1), c = k - r * (TX + 1);
+        int i = t.i0 + r, j = t.j0 + c;
+        T etaH = T(0.25) * (s_etaH[r][c] + s_etaH[r][c + 1] + s_etaH[r + 1][c] + s_etaH[r + 1][c + 1]);
+        s_sxy[r][c] = shear_stress(U(i - 1, j), U(i, j), V(i, j - 1), V(i, j), etaH, dxi,
+                                   i > 0 && i < ny && j > 0 && j < nx).res;
+    }
+    __syncthreads();
+
+    // phase 3: owned outputs
+#pragma unroll
+    for (int k = 0; k < RPT; k++) {
+        const int r = t.ty + k * (NTHR / TX);
+        const int c = t.tx;
+        const int i = t.i0 + r, j = t.j0 + c;
+        if (i >= ny || j >= nx) continue;
+        const int sr = r + 1, sc = c + 1;  // this cell in the staged cell windows
+        const T Hc = s_H[sr][sc], Hl = s_H[sr][sc - 1], Hr = s_H[sr][sc + 1];
+        const T Ht = s_H[sr - 1][sc], Hb = s_H[sr + 1][sc];
+        const T bc = s_bed[sr][sc], bl = s_bed[sr][sc - 1], bt = s_bed[sr - 1][sc];
+        const T betac = s_beta[sr][sc], betal = s_beta[sr][sc - 1], betat = s_beta[sr - 1][sc];
+        const T ul = U(i, j), ur = U(i, j + 1), vt = V(i, j), vb = V(i + 1, j);
+        const int64_t ic = int64_t(i) * nx + j;
+
+        // ---- mass row (residuals.cu:50-84)
+        {
+            const T m = mask[ic];
+            Flux<T> ql = upwind_flux(ul, Hl, Hc, j > 0 && j < nx);
+            Flux<T> qr = upwind_flux(ur, Hc, Hr, j + 1 > 0 && j + 1 < nx);
+            Flux<T> qt = upwind_flux(vt, Hc, Ht, i > 0 && i < ny);
+            Flux<T> qb = upwind_flux(vb, Hb, Hc, i + 1 > 0 && i + 1 < ny);
+            Calving<T> cv = calving(Hc, bc, p);
+            T rH = Hc / p.dt - f_H[ic];
+            rH -= cv.res;
+            rH -= ql.res * dxi;
+            rH += qr.res * dxi;
+            rH += qt.res * dxi;
+            rH -= qb.res * dxi;
+            o_H[ic] = (T(1) - m) * rH + m * (Hc - gamma[ic]);
+        }
+        // ---- u-face (i,j) and, at the right edge, (i,nx)
+        for (int e = 0; e < 2; e++) {
+            const int jj = j + e;
+            if (e == 1 && jj != nx) break;
+            const int cc = c + e;
+            T val = (s_sxx[r][cc + 1] - s_sxx[r][cc]) * dxi + (s_sxy[r][cc] - s_sxy[r + 1][cc]) * dxi;
+            const T uf = e ? ur : ul;
+            const T H1 = e ? Hc : Hl, H2 = e ? Hr : Hc;
+            const T b1 = e ? bc : bl, b2 = e ? s_bed[sr][sc + 1] : bc;
+            const T be1 = e ? betac : betal, be2 = e ? s_beta[sr][sc + 1] : betac;
+            BasalDrag<T> tb = basal_drag(uf, H1, H2, b1, b2, be1, be2, p);
+            Driving<T> td = driving(H1, H2, b1, b2, dxi, jj > 0 && jj < nx);
+            val += tb.res - td.res;
+            val -= f_u[int64_t(i) * (nx + 1) + jj];
+            o_u[int64_t(i) * (nx + 1) + jj] = val;
+        }
+        // ---- v-face (i,j) and, at the bottom edge, (ny,j)
+        for (int e = 0; e < 2; e++) {
+            const int ii = i + e;
+            if (e == 1 && ii != ny) break;
+            const int rr = r + e;
+            T val = (s_syy[rr][c] - s_syy[rr + 1][c]) * dxi + (s_sxy[rr][c + 1] - s_sxy[rr][c]) * dxi;
+            const T vf = e ? vb : vt;
+            const T Htop = e ? Hc : Ht, Hbot = e ? Hb : Hc;
+            const T btop = e ? bc : bt, bbot = e ? s_bed[sr + 1][sc] : bc;
+            const T betop = e ? betac : betat, bebot = e ? s_beta[sr + 1][sc] : betac;
+            BasalDrag<T> tb = basal_drag(vf, Htop, Hbot, btop, bbot, betop, bebot, p);
+            Driving<T> td = driving(Hbot, Htop, bbot, btop, dxi, ii > 0 && ii < ny);
+            val += tb.res - td.res;
+            val -= f_v[int64_t(ii) * nx + j];
+            o_v[int64_t(ii) * nx + j] = val;
+        }
+    }
+}
+
 constexpr int VTY = 8;                   // VJP tile rows (keeps FP64 shared memory < 48 KB)
 constexpr int VRPT = VTY / (NTHR / TX);  // rows per thread = 1
 constexpr int VWR = VTY + 2;
@@ -485,7 +644,7 @@ int launch_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, c
                     void* r_H, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    glide::count_launch(), stencil_kernel<T, false><<<tile_grid(g), NTHR, 0, s>>>(
+    glide::count_launch(), residual_kernel<T><<<tile_grid(g), NTHR, 0, s>>>(
         (T*)r_u, (T*)r_v, (T*)r_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
         (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
         (const T*)a->gamma, g, p);
