@@ -23,7 +23,7 @@ SYMBOLS = [
     "glide_mask_le", "glide_convert", "glide_norms", "glide_norm_parts", "glide_fascd_vcycle",
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
     "glide_graph_destroy", "glide_launch_count", "glide_version", "glide_vanka_sweeps_noalloc",
-    "glide_noalloc_scratch_bytes", "glide_vanka_sweeps_ex",
+    "glide_noalloc_scratch_bytes", "glide_vanka_sweeps_ex", "glide_vanka_lu", "glide_vanka_linear",
 ]
 
 
@@ -86,6 +86,8 @@ def load():
         "glide_grad_beta": [LA, vp, vp, vp, i, vp],
         "glide_vanka_sweeps": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp, vp],
         "glide_vanka_sweeps_ex": [LA, vp, vp, vp, i, i, d, d, d, vp, vp, vp, vp],
+        "glide_vanka_lu": [LA, vp, vp, d, vp],
+        "glide_vanka_linear": [LA, vp, vp, vp, vp, vp, vp, vp, d, vp, vp],
         "glide_vanka_cells": [LA, vp, vp, vp, i, i, d, vp, vp, vp, vp],
         "glide_error_mask": [LA, vp, vp, vp, d, vp, vp, vp, vp],
         "glide_tile_flags": [LA, vp, vp, vp, vp],

@@ -21,6 +21,8 @@ template <typename T> int launch_jvp(const GlideLevelArgs*, const void*, const v
 template <typename T> int launch_vjp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*, void*, void*, void*, int, cudaStream_t);
 template <typename T> int launch_grad_beta(const GlideLevelArgs*, const void*, const void*, void*, int, cudaStream_t);
 template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t, double);
+template <typename T> int launch_vanka_lu(const GlideLevelArgs*, const void*, void*, double, cudaStream_t);
+template <typename T> int launch_vanka_linear(const GlideLevelArgs*, const void*, const void*, const void*, const void*, void*, void*, void*, double, void*, cudaStream_t);
 template <typename T> int launch_vanka_cells(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, const int*, const int*, void*, cudaStream_t, double);
 template <typename T> int launch_error_mask(const GlideLevelArgs*, const void*, const void*, const void*, double, void*, int*, int*, cudaStream_t);
 template <typename T> int launch_tile_flags(const GlideLevelArgs*, const void*, int*, int*, cudaStream_t);
@@ -124,6 +126,25 @@ int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v
                        void* scratch, void* stream) {
     return glide_vanka_sweeps_ex(a, f_u, f_v, f_H, n_iter, n_newton, GLIDE_REF_NEWTON_STEP, omega, shift, flags,
                                  any_active, scratch, stream);
+}
+
+int glide_vanka_lu(const GlideLevelArgs* a, const void* f_H, void* lu, double shift, void* stream) {
+    int e = check_level(a);
+    if (e) return e;
+    if (!lu || !f_H) return GLIDE_E_NULL;
+    return TDISPATCH(a->dtype, launch_vanka_lu<float>(a, f_H, lu, shift, S(stream)),
+                     launch_vanka_lu<double>(a, f_H, lu, shift, S(stream)));
+}
+
+int glide_vanka_linear(const GlideLevelArgs* a, const void* rho_u, const void* rho_v, const void* rho_H,
+                       const void* lu, void* d_u, void* d_v, void* d_H, double omega, void* scratch, void* stream) {
+    int e = check_level(a);
+    if (e) return e;
+    if (!rho_u || !rho_v || !rho_H || !lu || !d_u || !d_v || !d_H || !scratch) return GLIDE_E_NULL;
+    return TDISPATCH(a->dtype,
+                     launch_vanka_linear<float>(a, rho_u, rho_v, rho_H, lu, d_u, d_v, d_H, omega, scratch, S(stream)),
+                     launch_vanka_linear<double>(a, rho_u, rho_v, rho_H, lu, d_u, d_v, d_H, omega, scratch,
+                                                 S(stream)));
 }
 
 int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,

@@ -479,6 +479,115 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BL
     scratch[4 * nc + ic] = Hc - H0;
 }
 
+// --------------------------------------------------------------------------
+// Linear Vanka for defect correction (no counterpart in the reference): the
+// local 5x5 matrix of each cell at the current state (the same matrix the
+// first Newton iteration of vanka_cells_kernel factors) is factored once and
+// stored; each sweep then solves it against the cell's part of the linear
+// residual rho = r + J d, giving the additive-Vanka update of the correction
+// d with the H >= gamma bound applied to H + d_H.
+// --------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void lu5_factor(T (&A)[25]) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const T inv = T(1) / A[k * 5 + k];
+#pragma unroll
+        for (int i = k + 1; i < 5; i++) {
+            A[i * 5 + k] *= inv;
+#pragma unroll
+            for (int j = k + 1; j < 5; j++) A[i * 5 + j] -= A[i * 5 + k] * A[k * 5 + j];
+        }
+        A[k * 5 + k] = inv;  // stored as the reciprocal pivot
+    }
+}
+template <typename T>
+__device__ __forceinline__ void lu5_subst(const T (&A)[25], const T (&b)[5], T (&x)[5]) {
+    T y1 = b[1] - A[5] * b[0];
+    T y2 = b[2] - A[10] * b[0] - A[11] * y1;
+    T y3 = b[3] - A[15] * b[0] - A[16] * y1 - A[17] * y2;
+    T y4 = b[4] - A[20] * b[0] - A[21] * y1 - A[22] * y2 - A[23] * y3;
+    x[4] = y4 * A[24];
+    x[3] = (y3 - A[19] * x[4]) * A[18];
+    x[2] = (y2 - A[13] * x[3] - A[14] * x[4]) * A[12];
+    x[1] = (y1 - A[7] * x[2] - A[8] * x[3] - A[9] * x[4]) * A[6];
+    x[0] = (b[0] - A[1] * x[1] - A[2] * x[2] - A[3] * x[3] - A[4] * x[4]) * A[0];
+}
+
+// lu[k * nc + cell], k = 0..24: factors of the cell's local matrix at U.
+template <typename T>
+__global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BLOCKS) vanka_lu_kernel(
+    T* __restrict__ lu, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
+    const T* __restrict__ f_H, const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
+    const T* __restrict__ gamma, T shift, Geo g, Phys<T> p) {
+    __shared__ T s_eta[VY + 2][VX + 2];
+    const int ny = g.ny, nx = g.nx;
+    const int bz = blockIdx.z;
+    u += bz * g.nu(); v += bz * g.nv(); H += bz * g.nc(); f_H += bz * g.nc();
+    bed += bz * g.nc(); B += bz * g.nc(); beta += bz * g.nc(); gamma += bz * g.nc();
+    const int64_t nc = g.nc();
+    lu += bz * 25 * nc;
+    const int i0 = blockIdx.y * VY, j0 = blockIdx.x * VX;
+    const int r = threadIdx.x / VX, c = threadIdx.x % VX;
+    const int i = i0 + r, j = j0 + c;
+    eta_window(s_eta, u, v, B, i0, j0, ny, nx, p);
+    __syncthreads();
+    if (i >= ny || j >= nx) return;
+    Frozen<T> F;
+    {
+        Patch<T> P;
+        load_patch(P, s_eta, r, c, u, v, H, bed, beta, i, j, ny, nx, p);
+        make_frozen(F, P, ny, nx, p);
+    }
+    const int64_t ic = int64_t(i) * nx + j;
+    const T ul = u[int64_t(i) * (nx + 1) + j], ur = u[int64_t(i) * (nx + 1) + j + 1];
+    const T vt = v[ic], vb = v[int64_t(i + 1) * nx + j];
+    T J[25], rr[5];
+    // the momentum rows do not depend on f; the mass row's active-set switch
+    // (vanka.cu:104-113) needs the local mass residual, hence f_H
+    assemble_fast<T>(F, ul, ur, vt, vb, H[ic], T(0), T(0), T(0), T(0), f_H[ic], gamma[ic], T(1) / p.dt, p, J, rr);
+    J[0] -= shift; J[6] -= shift; J[12] -= shift; J[18] -= shift; J[24] += shift;  // vanka.cu:406-410
+    lu5_factor(J);
+#pragma unroll
+    for (int k = 0; k < 25; k++) lu[k * nc + ic] = J[k];
+}
+
+// scratch = the additive-Vanka halves of -A^-1 rho (same layout as
+// vanka_cells_kernel), with H + d_H + delta_H >= gamma.
+template <typename T>
+__global__ void vanka_linear_kernel(T* __restrict__ scratch, const T* __restrict__ lu,
+                                    const T* __restrict__ rho_u, const T* __restrict__ rho_v,
+                                    const T* __restrict__ rho_H, const T* __restrict__ H,
+                                    const T* __restrict__ dH, const T* __restrict__ gamma, Geo g) {
+    const int ny = g.ny, nx = g.nx;
+    const int bz = blockIdx.z;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= ny || j >= nx) return;
+    const int64_t nc = g.nc();
+    rho_u += bz * g.nu(); rho_v += bz * g.nv(); rho_H += bz * nc; H += bz * nc; dH += bz * nc;
+    gamma += bz * nc; lu += bz * 25 * nc; scratch += bz * 5 * nc;
+    const int64_t ic = int64_t(i) * nx + j;
+    T A[25];
+#pragma unroll
+    for (int k = 0; k < 25; k++) A[k] = lu[k * nc + ic];
+    const T b[5] = {rho_u[int64_t(i) * (nx + 1) + j], rho_u[int64_t(i) * (nx + 1) + j + 1], rho_v[ic],
+                    rho_v[int64_t(i + 1) * nx + j], rho_H[ic]};
+    T x[5];
+    lu5_subst(A, b, x);
+    T dHc = -x[4];
+    dHc = M<T>::max(dHc, gamma[ic] - H[ic] - dH[ic]);
+    if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(x[3]) && isfinite(dHc))) {
+        x[0] = x[1] = x[2] = x[3] = T(0);
+        dHc = T(0);
+    }
+    scratch[ic] = T(-0.5) * x[0];
+    scratch[nc + ic] = T(-0.5) * x[1];
+    scratch[2 * nc + ic] = T(-0.5) * x[2];
+    scratch[3 * nc + ic] = T(-0.5) * x[3];
+    scratch[4 * nc + ic] = dHc;
+}
+
 // U += omega * delta, face delta = sum of the two adjacent cells' halves.
 template <typename T, bool LOCAL>
 __global__ void vanka_apply_kernel(T* __restrict__ u, T* __restrict__ v, T* __restrict__ H,
@@ -657,6 +766,33 @@ int launch_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v
 }
 
 template <typename T>
+int launch_vanka_lu(const GlideLevelArgs* a, const void* f_H, void* lu, double shift, cudaStream_t s) {
+    Geo g{a->ny, a->nx, a->nb};
+    Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
+    glide::count_launch(), vanka_lu_kernel<T><<<cell_grid(g), VNT, 0, s>>>(
+        (T*)lu, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_H, (const T*)a->bed, (const T*)a->B,
+        (const T*)a->beta, (const T*)a->gamma, T(shift), g, p);
+    return (int)cudaGetLastError();
+}
+
+// d += omega * (linear Vanka update of rho), n_iter times with a fixed rho is
+// not useful: one sweep per call, rho recomputed by the caller in between.
+template <typename T>
+int launch_vanka_linear(const GlideLevelArgs* a, const void* rho_u, const void* rho_v, const void* rho_H,
+                        const void* lu, void* d_u, void* d_v, void* d_H, double omega, void* scratch,
+                        cudaStream_t s) {
+    Geo g{a->ny, a->nx, a->nb};
+    dim3 blk(32, 8);
+    dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, g.nb);
+    glide::count_launch(), vanka_linear_kernel<T><<<grd, blk, 0, s>>>(
+        (T*)scratch, (const T*)lu, (const T*)rho_u, (const T*)rho_v, (const T*)rho_H, (const T*)a->H,
+        (const T*)d_H, (const T*)a->gamma, g);
+    glide::count_launch(), vanka_apply_kernel<T, false><<<face_grid(g), dim3(32, 8), 0, s>>>(
+        (T*)d_u, (T*)d_v, (T*)d_H, (const T*)scratch, nullptr, nullptr, T(omega), g);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
 int launch_error_mask(const GlideLevelArgs* a, const void* r_u, const void* r_v, const void* r_H, double threshold,
                       void* err_mask, int* flags, int* any_active, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
@@ -702,7 +838,10 @@ int launch_vanka_adjoint(const GlideLevelArgs* a, void* l_u, void* l_v, void* l_
                                       void*, int*, int*, cudaStream_t);                                           \
     template int launch_tile_flags<T>(const GlideLevelArgs*, const void*, int*, int*, cudaStream_t);              \
     template int launch_vanka_adjoint<T>(const GlideLevelArgs*, void*, void*, void*, const void*, const void*,    \
-                                         const void*, int, double, cudaStream_t);
+                                         const void*, int, double, cudaStream_t);                                 \
+    template int launch_vanka_lu<T>(const GlideLevelArgs*, const void*, void*, double, cudaStream_t);             \
+    template int launch_vanka_linear<T>(const GlideLevelArgs*, const void*, const void*, const void*, const void*, \
+                                        void*, void*, void*, double, void*, cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

@@ -205,6 +205,26 @@ class Grid:
         self.update_tile_flags()
         self._sweeps(n_iter, n_inner, omega, shift, True, step)
 
+    def vanka_lu(self, shift=1.0):
+        """Factor every cell's local Vanka matrix at the current state with
+        right-hand side f (for linear sweeps); the factors stay in this grid
+        until the next call."""
+        if getattr(self, "_lu", None) is None:
+            self._lu = torch.empty(25 * self.nb * self.nh, dtype=self.dtype, device=self.device)
+        a = self.level_args()
+        N.check(self._lib.glide_vanka_lu(C.byref(a), self.f_H.data_ptr(), self._lu.data_ptr(), float(shift),
+                                         self._s()), "vanka lu")
+
+    def vanka_linear_sweep(self, rho, d, omega=0.5):
+        """d += omega * additive linear Vanka update for the linear residual
+        rho = r + J d (rho, d: monolithic vectors like U)."""
+        ru, rv, rH = self._vec_to_fields(rho)
+        du, dv, dH = self._vec_to_fields(d)
+        a = self.level_args()
+        N.check(self._lib.glide_vanka_linear(C.byref(a), ru.data_ptr(), rv.data_ptr(), rH.data_ptr(),
+                                             self._lu.data_ptr(), du.data_ptr(), dv.data_ptr(), dH.data_ptr(),
+                                             float(omega), self._scratch.data_ptr(), self._s()), "vanka linear")
+
     def vanka_smooth_adjoint(self, color, omega=0.5):
         """One adjoint colour update from the current r_adj (glide/grid.py:286-303)."""
         a = self.level_args()

@@ -61,7 +61,7 @@ class IcePhysics:
                  gl_sigmoid_c=0.1, gl_derivatives=False, *, precision="fp32", device=None,
                  settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0,
                  stall_factor=0.5, finish_block=20, finish_anderson=0, finish_fp32=False, finish_newton=None,
-                 finish_step=None):
+                 finish_step=None, finish_linear=False, finish_patience=3):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -83,6 +83,8 @@ class IcePhysics:
         self.finish_fp32 = bool(finish_fp32)
         self.finish_newton = None if finish_newton is None else int(finish_newton)
         self.finish_step = None if finish_step is None else float(finish_step)
+        self.finish_linear = bool(finish_linear)
+        self.finish_patience = int(finish_patience)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
         self.dtype = _PRECISIONS[precision]
@@ -338,6 +340,12 @@ class IcePhysics:
         correction problem f32 = F32(fl32(U64)) - r64 while they still cut the
         FP64 residual, then FP64 sweeps.  ``finish_anderson`` = m > 0 applies
         Anderson acceleration (depth m) over the blocks to the velocity part.
+        ``finish_linear``: the FP32 blocks solve the linearised correction
+        problem instead (``_linear_block``) and hand over to FP64 after
+        ``finish_patience`` blocks without a new best.  Ten blocks without
+        progress restore the best state and continue in FP64 with the
+        reference's damped local Newton and no extrapolation; a second
+        stagnation ends the finish.
         """
         g = self.grid
         st = self.settings
@@ -353,9 +361,14 @@ class IcePhysics:
         good.copy_(g.U)
         since_best = 0
         local = self._finish_local()
+        blocks = {"fp32": 0, "fp64": 0}
+        info["finish_blocks"] = blocks
         while done < max_sweeps and rel > tol:
             x0 = g.U[:nU].clone() if m > 0 else None
-            if use32:
+            blocks["fp32" if use32 else "fp64"] += 1
+            if use32 and self.finish_linear:
+                self._linear_block(self.finish_block)
+            elif use32:
                 self._fp32_sweeps(self.finish_block, local)
             else:
                 g.vanka_sweep(self.finish_block, omega=st.omega, shift=st.shift, **local)
@@ -371,7 +384,9 @@ class IcePhysics:
                 if len(Fs) > 1:
                     dF = torch.stack([Fs[k + 1] - Fs[k] for k in range(len(Fs) - 1)], 1)
                     dG = torch.stack([Gs[k + 1] - Gs[k] for k in range(len(Gs) - 1)], 1)
-                    # least squares min |f - dF gam| via the (tiny) normal equations
+                    # least squares min |f - dF gam| via the (tiny) normal equations; an extrapolation that
+                    # raises |r| is kept on purpose: measured, it shortens the finish (the residual norm
+                    # understates the smooth error it removes)
                     Gm = dF.T @ dF
                     Gm = Gm + 1e-12 * torch.trace(Gm) * torch.eye(Gm.shape[0], dtype=Gm.dtype, device=Gm.device)
                     gam = torch.linalg.solve(Gm, dF.T @ f)
@@ -397,11 +412,27 @@ class IcePhysics:
                 best = rel
                 good.copy_(g.U)
             since_best += 1
-            if since_best > 10:   # no progress over 10 blocks: stop (a late guess fallback may follow)
-                info["finish_stagnated"] = True
-                break
-            if use32 and rel > 0.7 * prev:
-                use32 = False           # FP32 correction floor reached: continue in FP64
+            if since_best > 10:
+                # no progress over 10 blocks: back to the best state and on in FP64 with the reference's
+                # damped local Newton and no extrapolation; a second stagnation ends the finish (a late
+                # guess fallback may follow)
+                safe = dict(n_inner=REFERENCE.n_newton, step=REFERENCE.newton_step)
+                if local == safe and not use32 and m == 0:
+                    info["finish_stagnated"] = True
+                    break
+                g.U.copy_(good)
+                rel = best
+                local, use32, m = safe, False, 0
+                Fs, Gs = [], []
+                since_best = 0
+                info["finish_safe"] = True
+                continue
+            # the FAS-form FP32 correction floors near eps32 x |operator terms|: hand over to FP64 once a
+            # block gains little; the linear form has no such floor and hands over only when it has not
+            # set a new best for finish_patience blocks (Anderson steps may raise |r| for a while)
+            if use32 and ((self.finish_linear and since_best >= self.finish_patience) or
+                          (not self.finish_linear and rel > 0.7 * prev)):
+                use32 = False
                 Fs, Gs = [], []
             prev = rel
         info["finish_sweeps"] = done
@@ -419,6 +450,38 @@ class IcePhysics:
         if getattr(self, "_good", None) is None or self._good.shape != self.grid.U.shape:
             self._good = torch.empty_like(self.grid.U)
         return self._good
+
+    def _linear_block(self, n):
+        """Defect correction in linear form: r64 = F64(U64) - f64; n FP32
+        additive Vanka sweeps for r + J d = 0 linearised at fl32(U64) (local
+        matrices factored once, J d from the FP32 JVP kernel); U64 += fl64(d).
+        Unlike the FAS-form correction its rounding error scales with d, not
+        with the size of the operator's terms."""
+        g64, g32 = self.grid, self.grid32
+        lib = self.kernels
+        s = N.stream_handle()
+        st = self.settings
+        ntot = g64.nb * g64.n_total
+        g64.compute_residual()
+        N.check(lib.glide_convert(N.F32, g32.U.data_ptr(), g64.U.data_ptr(), ntot, 0, s), "convert")
+        N.check(lib.glide_convert(N.F32, g32.r.data_ptr(), g64.r.data_ptr(), ntot, 0, s), "convert")
+        g32.gamma.fill_(self.thklim)
+        # f32 = F32(U32) - r: the local mass residual of the factorisation equals r_H
+        a = g32.level_args()
+        N.check(lib.glide_residual(C.byref(a), g32.r_u.data_ptr(), g32.r_v.data_ptr(), g32.r_H.data_ptr(),
+                                   g32.f_u.data_ptr(), g32.f_v.data_ptr(), g32.f_H.data_ptr(), s), "residual32")
+        g32.vanka_lu(st.shift)
+        g32.d_U.zero_()
+        for k in range(n):
+            if k == 0:
+                rho = g32.r
+            else:
+                g32.compute_jvp()
+                N.check(lib.glide_lincomb(N.F32, g32.z.data_ptr(), g32.r.data_ptr(), 1.0, g32.j.data_ptr(), 1.0,
+                                          ntot, s), "lincomb")
+                rho = g32.z
+            g32.vanka_linear_sweep(rho, g32.d_U, st.omega)
+        N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.d_U.data_ptr(), ntot, 1, s), "convert")
 
     def _fp32_sweeps(self, n, local=None):
         """FP32 fine-level sweeps on the FP64 problem's correction equation."""

@@ -109,6 +109,18 @@ int glide_vanka_sweeps_noalloc(const GlideLevelArgs* a, const void* f_u, const v
                                int n_newton, double omega, double shift, const int* flags, const int* any_active,
                                void* stream);
 size_t glide_noalloc_scratch_bytes(void);
+/* Linear Vanka for defect correction (no counterpart in the reference: the
+ * tolerance solver's FP32 correction of an FP64 state).  glide_vanka_lu
+ * factors every cell's local 5x5 matrix at the state in a (the matrix of the
+ * first local Newton iteration of glide_vanka_sweeps with right-hand side
+ * f_H in the mass row's active-set test, diagonal shifted by shift) into lu
+ * (25 * ny * nx * nb elements).  glide_vanka_linear makes one
+ * additive sweep for the correction d of the linear problem r + J d = 0:
+ * rho = r + J d is the caller's linear residual; d += omega * (face average
+ * of -A^-1 rho), with H + d_H kept >= gamma.  scratch as for the sweeps. */
+int glide_vanka_lu(const GlideLevelArgs* a, const void* f_H, void* lu, double shift, void* stream);
+int glide_vanka_linear(const GlideLevelArgs* a, const void* rho_u, const void* rho_v, const void* rho_H,
+                       const void* lu, void* d_u, void* d_v, void* d_H, double omega, void* scratch, void* stream);
 /* Only the per-cell local Newton kernel of a sweep, n_launch times, writing the
  * per-cell deltas into scratch without updating U (profiling and timing). */
 int glide_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_launch,

@@ -290,6 +290,34 @@ def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt,
     return du, dv, dH
 
 
+def vanka_linear_update(u, v, H, f_H, rho_u, rho_v, rho_H, d_H, bed, B, beta, gamma, p: Params, dx, dt,
+                        shift=1.0):
+    """One additive linear Vanka update for r + J d = 0 (test oracle of the
+    extension entry point glide_vanka_linear, which has no counterpart in the
+    reference).  Every cell solves its local matrix at (u, v, H) -- the matrix
+    of the first local Newton iteration of vanka_deltas, with the same
+    diagonal shift and with f_H in the mass row's active-set test -- against
+    rho at its 4 faces and its cell; faces receive
+    half of each adjacent cell's update, H the whole of it, bounded so that
+    H + d_H + delta_H >= gamma.  Returns (du, dv, dH) before the omega factor.
+    """
+    ny, nx = H.shape
+    fz = _Frozen(u, v, H, bed, B, beta, p, dx)
+    zu, zv = np.zeros((ny, nx + 1)), np.zeros((ny + 1, nx))
+    Jm, _ = _assemble(fz, fz.U(0, 0), fz.U(0, 1), fz.V(0, 0), fz.V(1, 0), H.copy(), p, dx, dt, True, (zu, zv, f_H),
+                      gamma)
+    Jm[0] -= shift; Jm[6] -= shift; Jm[12] -= shift; Jm[18] -= shift; Jm[24] += shift
+    b = [rho_u[:, :nx], rho_u[:, 1:], rho_v[:ny], rho_v[1:], rho_H]
+    x = lu5_solve(Jm, b)
+    dH = np.maximum(-x[4], gamma - H - d_H)
+    du = np.zeros((ny, nx + 1)); dv = np.zeros((ny + 1, nx))
+    du[:, :nx] += -0.5 * x[0]
+    du[:, 1:] += -0.5 * x[1]
+    dv[:ny, :] += -0.5 * x[2]
+    dv[1:, :] += -0.5 * x[3]
+    return du, dv, dH
+
+
 def local_cell_on(error_mask):
     """Cells updated by ``vanka_smooth_local`` (vanka.cu:875-888).
 
