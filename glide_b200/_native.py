@@ -24,6 +24,7 @@ SYMBOLS = [
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
     "glide_graph_destroy", "glide_launch_count", "glide_version", "glide_vanka_sweeps_noalloc",
     "glide_noalloc_scratch_bytes", "glide_vanka_sweeps_ex", "glide_vanka_lu", "glide_vanka_linear",
+    "glide_misfit", "glide_tikhonov", "glide_loss_parts",
 ]
 
 
@@ -87,6 +88,9 @@ def load():
         "glide_vanka_sweeps": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp, vp],
         "glide_vanka_sweeps_ex": [LA, vp, vp, vp, i, i, d, d, d, vp, vp, vp, vp],
         "glide_vanka_lu": [LA, vp, vp, d, vp],
+        "glide_misfit": [i, i, d, vp, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp],
+        "glide_tikhonov": [i, vp, i, i, vp, vp, vp, vp],
+        "glide_loss_parts": [i64],
         "glide_vanka_linear": [LA, vp, vp, vp, vp, vp, vp, vp, d, vp, vp],
         "glide_vanka_cells": [LA, vp, vp, vp, i, i, d, vp, vp, vp, vp],
         "glide_error_mask": [LA, vp, vp, vp, d, vp, vp, vp, vp],

@@ -33,10 +33,8 @@ import numpy as np
 import torch
 
 from .kernels import prolongate_cell_centered, restrict_hfacet, restrict_vfacet
-from .physics import abs_grad, abs_loss, huber_grad, huber_loss, tikhonov_regularization
+from .losses import KINDS, misfit, tikhonov
 from .solver import adjoint_vcycle, fascd_vcycle, restrict_parameters_to_hierarchy
-
-LOSSES = {"abs": (abs_loss, abs_grad), "huber": (huber_loss, huber_grad)}
 
 
 def observation_hierarchy(physics, u_obs, v_obs):
@@ -65,7 +63,9 @@ class LevelObjective:
         self.u_obs, self.v_obs = u_obs, v_obs
         self.dt = float(dt)
         self.reg_weight = float(reg_weight)
-        self.loss, self.loss_grad = LOSSES[loss]
+        if loss not in KINDS:
+            raise ValueError(f"loss must be one of {sorted(KINDS)}")
+        self.loss = loss
         self.n_vcycles, self.n_adjoint = int(n_vcycles), int(n_adjoint_vcycles)
         self.tol, self.adj_tol, self.exact = tol, adj_tol, bool(exact)
         self.consistent_reg = bool(consistent_reg)
@@ -112,11 +112,11 @@ class LevelObjective:
         log_beta = torch.as_tensor(np.asarray(x, dtype=np.float64).reshape(g.ny, g.nx), device=g.device)
         g.beta.copy_(torch.exp(log_beta).to(g.dtype))
         self._forward(g)
-        J = float(self.loss(g.u, g.v, self.u_obs, self.v_obs))
-        du, dv = self.loss_grad(g.u, g.v, self.u_obs, self.v_obs)
-        grad_beta = self._adjoint(g, du.to(g.dtype), dv.to(g.dtype))
+        J_dev, du, dv = misfit(g.u, g.v, self.u_obs, self.v_obs, kind=self.loss)   # fused loss + gradient
+        grad_beta = self._adjoint(g, du, dv)
         grad = g.beta * grad_beta
-        tik, tik_grad = tikhonov_regularization(g.beta)
+        tik_dev, tik_grad = tikhonov(g.beta)
+        J, tik = float(J_dev), float(tik_dev)
         if self.consistent_reg:
             tik_grad = tik_grad * g.beta
         total = J + self.reg_weight * tik

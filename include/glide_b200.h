@@ -205,6 +205,22 @@ int glide_graph_create(GlideLevel* levels, int n_levels, const GlideSolverConfig
 int glide_graph_launch(void* graph, void* stream);
 int glide_graph_destroy(void* graph);
 
+/* ---- fused loss kernels for the inverse problem (glide/physics.py:262-411) -- */
+/* Misfit of (u, v) against (u_obs, v_obs) and its gradient in one pass,
+ * NaN differences counted as 0; kind 0: mean |d| per component (abs_loss /
+ * abs_grad), kind 1: mean sqrt(d^2 + eps) (huber_loss / huber_grad); both
+ * gradients divide by nu as the reference's helpers do.  out3 (device
+ * double[3]) = {L_u + L_v, sum_u, sum_v}; parts: glide_loss_parts(max(nu, nv))
+ * doubles.  Deterministic. */
+int glide_misfit(int dtype, int kind, double eps, const void* u, const void* v, const void* u_obs,
+                 const void* v_obs, int64_t nu, int64_t nv, void* grad_u, void* grad_v, double* out3, double* parts,
+                 void* stream);
+/* Tikhonov term 1/2 sum (neighbour differences)^2 of an (ny, nx) field and
+ * its gradient (tikhonov_regularization); out1 = device double[1]. */
+int glide_tikhonov(int dtype, const void* field, int ny, int nx, void* grad, double* out1, double* parts,
+                   void* stream);
+int glide_loss_parts(int64_t n);
+
 /* ---- learned initial guess (no counterpart in the reference) -------------- */
 /* C[M,N] (+)= A[M,K] * B[N,K]^T on the tcgen05 tensor cores: A, B BF16 row-major
  * with K contiguous (lda, ldb >= K, 16-byte aligned rows for the fast path),
