@@ -59,7 +59,7 @@ class SolverConfig(C.Structure):
                 ("n_local", C.c_int), ("n_newton", C.c_int), ("omega", C.c_double), ("shift", C.c_double),
                 ("err_threshold", C.c_double), ("adj_coarse", C.c_int), ("adj_smooth", C.c_int),
                 ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int),
-                ("newton_step", C.c_double), ("coarse_line_search", C.c_int)]
+                ("newton_step", C.c_double), ("pivoted_lu", C.c_int), ("coarse_line_search", C.c_int)]
 
 
 class NativeError(RuntimeError):
@@ -86,7 +86,7 @@ def load():
         "glide_vjp": [LA, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp],
         "glide_grad_beta": [LA, vp, vp, vp, i, vp],
         "glide_vanka_sweeps": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp, vp],
-        "glide_vanka_sweeps_ex": [LA, vp, vp, vp, i, i, d, d, d, vp, vp, vp, vp],
+        "glide_vanka_sweeps_ex": [LA, vp, vp, vp, i, i, d, d, d, i, vp, vp, vp, vp],
         "glide_vanka_lu": [LA, vp, vp, d, vp],
         "glide_misfit": [i, i, d, vp, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp],
         "glide_tikhonov": [i, vp, i, i, vp, vp, vp, vp],

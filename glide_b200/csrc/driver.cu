@@ -20,7 +20,7 @@ template <typename T> int launch_residual(const GlideLevelArgs*, const void*, co
 template <typename T> int launch_jvp(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*, cudaStream_t);
 template <typename T> int launch_vjp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*, void*, void*, void*, int, cudaStream_t);
 template <typename T> int launch_grad_beta(const GlideLevelArgs*, const void*, const void*, void*, int, cudaStream_t);
-template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t, double);
+template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t, double, int);
 template <typename T> int launch_vanka_lu(const GlideLevelArgs*, const void*, void*, double, cudaStream_t);
 template <typename T> int launch_vanka_linear(const GlideLevelArgs*, const void*, const void*, const void*, const void*, void*, void*, void*, double, void*, cudaStream_t);
 template <typename T> int launch_vanka_cells(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, const int*, const int*, void*, cudaStream_t, double);
@@ -107,24 +107,25 @@ int glide_grad_beta(const GlideLevelArgs* a, const void* l_u, const void* l_v, v
 }
 
 int glide_vanka_sweeps_ex(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
-                          int n_newton, double newton_step, double omega, double shift, const int* flags,
-                          const int* any_active, void* scratch, void* stream) {
+                          int n_newton, double newton_step, double omega, double shift, int pivoted_lu,
+                          const int* flags, const int* any_active, void* scratch, void* stream) {
     int e = check_level(a);
     if (e) return e;
     if (!f_u || !f_v || !f_H || !scratch) return GLIDE_E_NULL;
     if ((flags == nullptr) != (any_active == nullptr)) return GLIDE_E_NULL;
     if (n_iter < 0 || n_newton < 0 || !(newton_step > 0.0 && newton_step <= 1.0)) return GLIDE_E_SHAPE;
+    const int pv = pivoted_lu ? 1 : 0;
     return TDISPATCH(a->dtype,
                      launch_vanka_sweeps<float>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags, any_active,
-                                                scratch, S(stream), newton_step),
+                                                scratch, S(stream), newton_step, pv),
                      launch_vanka_sweeps<double>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags,
-                                                 any_active, scratch, S(stream), newton_step));
+                                                 any_active, scratch, S(stream), newton_step, pv));
 }
 
 int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                        int n_newton, double omega, double shift, const int* flags, const int* any_active,
                        void* scratch, void* stream) {
-    return glide_vanka_sweeps_ex(a, f_u, f_v, f_H, n_iter, n_newton, GLIDE_REF_NEWTON_STEP, omega, shift, flags,
+    return glide_vanka_sweeps_ex(a, f_u, f_v, f_H, n_iter, n_newton, GLIDE_REF_NEWTON_STEP, omega, shift, 0, flags,
                                  any_active, scratch, stream);
 }
 
@@ -293,7 +294,8 @@ int vanka(GlideLevel* L, int n_iter, const GlideSolverConfig* c, bool local, voi
     LevelView w = view(L);
     const double step = c->newton_step > 0.0 ? c->newton_step : GLIDE_REF_NEWTON_STEP;
     return glide_vanka_sweeps_ex(&L->a, w.u(L->f), w.v(L->f), w.H(L->f), n_iter, c->n_newton, step, c->omega,
-                                 c->shift, local ? L->flags : nullptr, local ? L->any_active : nullptr, L->scratch, s);
+                                 c->shift, c->pivoted_lu, local ? L->flags : nullptr, local ? L->any_active : nullptr,
+                                 L->scratch, s);
 }
 
 int fill_gamma(GlideLevel* L, double val, void* s) {

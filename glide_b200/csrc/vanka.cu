@@ -413,6 +413,66 @@ template <typename T> __device__ __forceinline__ void lu5_solve_fast(T (&A)[25],
     x[0] = (b[0] - A[1] * x[1] - A[2] * x[2] - A[3] * x[3] - A[4] * x[4]) * inv[0];
 }
 
+// 5x5 solve with partial (row) pivoting, the robustness variant of the
+// reference (lu_5x5_solve_pivot, glide/cuda/common.cu:180-233): the largest
+// |entry| of the column becomes the pivot (first one on ties), a pivot below
+// 1e-14 in magnitude skips its elimination step, a diagonal below 1e-14 in
+// back substitution gives x = 0.  Rows are swapped in registers by unrolled
+// conditional moves.
+template <typename T> __device__ __forceinline__ void lu5_solve_pivot(T (&A)[25], const T (&b)[5], T (&x)[5]) {
+    T y[5] = {b[0], b[1], b[2], b[3], b[4]};
+    const T tiny = T(1e-14);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int p = k;
+        T best = M<T>::abs(A[k * 5 + k]);
+#pragma unroll
+        for (int i = k + 1; i < 5; i++) {
+            const T a = M<T>::abs(A[i * 5 + k]);
+            if (a > best) {
+                best = a;
+                p = i;
+            }
+        }
+#pragma unroll
+        for (int i = k + 1; i < 5; i++) {
+            if (i == p) {
+#pragma unroll
+                for (int j = 0; j < 5; j++) {
+                    const T t = A[k * 5 + j];
+                    A[k * 5 + j] = A[i * 5 + j];
+                    A[i * 5 + j] = t;
+                }
+                const T t = y[k];
+                y[k] = y[i];
+                y[i] = t;
+            }
+        }
+        const T piv = A[k * 5 + k];
+        if (M<T>::abs(piv) < tiny) continue;
+#pragma unroll
+        for (int i = k + 1; i < 5; i++) {
+            const T f = A[i * 5 + k] / piv;
+            A[i * 5 + k] = f;
+#pragma unroll
+            for (int j = k + 1; j < 5; j++) A[i * 5 + j] -= f * A[k * 5 + j];
+        }
+    }
+#pragma unroll
+    for (int i = 1; i < 5; i++) {
+#pragma unroll
+        for (int j = 0; j < i; j++) y[i] -= A[i * 5 + j] * y[j];
+    }
+#pragma unroll
+    for (int i = 4; i >= 0; i--) {
+        T v = y[i];
+#pragma unroll
+        for (int j = i + 1; j < 5; j++) v -= A[i * 5 + j] * x[j];
+        const T d = A[i * 5 + i];
+        x[i] = M<T>::abs(d) > tiny ? v / d : T(0);
+    }
+}
+
 // Per-cell Newton deltas.  scratch holds 5 cell arrays: 0.5*du_l, 0.5*du_r,
 // 0.5*dv_t, 0.5*dv_b, dH.
 template <typename T, bool LOCAL>
@@ -423,7 +483,7 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BL
     T* __restrict__ scratch, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, const T* __restrict__ bed,
     const T* __restrict__ B, const T* __restrict__ beta, const T* __restrict__ gamma, const int* __restrict__ flags,
-    const int* __restrict__ any_active, int n_newton, T shift, T step, Geo g, Phys<T> p) {
+    const int* __restrict__ any_active, int n_newton, T shift, T step, int pivot, Geo g, Phys<T> p) {
     __shared__ T s_eta[VY + 2][VX + 2];
     const int ny = g.ny, nx = g.nx;
     const int bz = blockIdx.z;
@@ -460,7 +520,10 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BL
         T J[25], rr[5], x[5];
         assemble_fast<T>(F, ul, ur, vt, vb, Hc, fu_l, fu_r, fv_t, fv_b, fH, thk, dti, p, J, rr);
         J[0] -= shift; J[6] -= shift; J[12] -= shift; J[18] -= shift; J[24] += shift;  // vanka.cu:406-410
-        lu5_solve_fast(J, rr, x);
+        if (pivot)
+            lu5_solve_pivot(J, rr, x);
+        else
+            lu5_solve_fast(J, rr, x);
         ul -= step * x[0];  // reference step 0.25: relaxation_factor, glide/cuda/vanka.cu:416
         ur -= step * x[1];
         vt -= step * x[2];
@@ -719,7 +782,7 @@ static inline dim3 face_grid(const Geo& g) { return dim3((g.nx + 1 + 31) / 32, (
 template <typename T>
 int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                         int n_newton, double omega, double shift, const int* flags, const int* any_active,
-                        void* scratch, cudaStream_t s, double newton_step) {
+                        void* scratch, cudaStream_t s, double newton_step, int pivot) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     T* u = (T*)a->u;
@@ -729,13 +792,13 @@ int launch_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_
         if (flags) {
             glide::count_launch(), vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, u, v, H, (const T*)f_u, (const T*)f_v, (const T*)f_H, (const T*)a->bed,
-                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags, any_active, n_newton, T(shift), T(newton_step), g, p);
+                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags, any_active, n_newton, T(shift), T(newton_step), pivot, g, p);
             glide::count_launch(), vanka_apply_kernel<T, true><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, flags,
                                                                                any_active, T(omega), g);
         } else {
             glide::count_launch(), vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, u, v, H, (const T*)f_u, (const T*)f_v, (const T*)f_H, (const T*)a->bed,
-                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr, nullptr, n_newton, T(shift), T(newton_step), g, p);
+                (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr, nullptr, n_newton, T(shift), T(newton_step), pivot, g, p);
             glide::count_launch(), vanka_apply_kernel<T, false><<<face_grid(g), dim3(32, 8), 0, s>>>(u, v, H, (const T*)scratch, nullptr,
                                                                                 nullptr, T(omega), g);
         }
@@ -755,12 +818,12 @@ int launch_vanka_cells(const GlideLevelArgs* a, const void* f_u, const void* f_v
             glide::count_launch(), vanka_cells_kernel<T, true><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
                 (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, flags,
-                any_active, n_newton, T(shift), T(newton_step), g, p);
+                any_active, n_newton, T(shift), T(newton_step), 0, g, p);
         else
             glide::count_launch(), vanka_cells_kernel<T, false><<<cell_grid(g), VNT, 0, s>>>(
                 (T*)scratch, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
                 (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->gamma, nullptr,
-                nullptr, n_newton, T(shift), T(newton_step), g, p);
+                nullptr, n_newton, T(shift), T(newton_step), 0, g, p);
     }
     return (int)cudaGetLastError();
 }
@@ -831,7 +894,7 @@ int launch_vanka_adjoint(const GlideLevelArgs* a, void* l_u, void* l_v, void* l_
 
 #define INST(T)                                                                                                  \
     template int launch_vanka_sweeps<T>(const GlideLevelArgs*, const void*, const void*, const void*, int, int,   \
-                                        double, double, const int*, const int*, void*, cudaStream_t, double);     \
+                                        double, double, const int*, const int*, void*, cudaStream_t, double, int);\
     template int launch_vanka_cells<T>(const GlideLevelArgs*, const void*, const void*, const void*, int, int,     \
                                        double, const int*, const int*, void*, cudaStream_t, double);              \
     template int launch_error_mask<T>(const GlideLevelArgs*, const void*, const void*, const void*, double,       \

@@ -30,7 +30,7 @@
 namespace glide {
 template <typename T>
 int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double,
-                        const int*, const int*, void*, cudaStream_t, double);
+                        const int*, const int*, void*, cudaStream_t, double, int);
 }
 
 namespace {
@@ -81,7 +81,7 @@ extern "C" int glide_vanka_sweeps_noalloc(const GlideLevelArgs* a, const void* f
     if (rc) return rc;
     return a->dtype == GLIDE_F32
                ? glide::launch_vanka_sweeps<float>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags, any_active,
-                                                   scratch, (cudaStream_t)stream, GLIDE_REF_NEWTON_STEP)
+                                                   scratch, (cudaStream_t)stream, GLIDE_REF_NEWTON_STEP, 0)
                : glide::launch_vanka_sweeps<double>(a, f_u, f_v, f_H, n_iter, n_newton, omega, shift, flags,
-                                                    any_active, scratch, (cudaStream_t)stream, GLIDE_REF_NEWTON_STEP);
+                                                    any_active, scratch, (cudaStream_t)stream, GLIDE_REF_NEWTON_STEP, 0);
 }

@@ -165,14 +165,14 @@ class Grid:
                                     self.lambda_H.data_ptr(), None, None, None, self.l_u.data_ptr(),
                                     self.l_v.data_ptr(), self.l_H.data_ptr(), int(exact_boundary), self._s()), "vjp")
 
-    def _sweeps(self, n_iter, n_inner, omega, shift, local, step=0.25):
+    def _sweeps(self, n_iter, n_inner, omega, shift, local, step=0.25, pivot=False):
         a = self.level_args()
         flags = self._flags.data_ptr() if local else None
         anyact = self._any_active.data_ptr() if local else None
         N.check(self._lib.glide_vanka_sweeps_ex(C.byref(a), self.f_u.data_ptr(), self.f_v.data_ptr(),
                                                 self.f_H.data_ptr(), int(n_iter), int(n_inner), float(step),
-                                                float(omega), float(shift), flags, anyact, self._scratch.data_ptr(),
-                                                self._s()), "vanka")
+                                                float(omega), float(shift), int(bool(pivot)), flags, anyact,
+                                                self._scratch.data_ptr(), self._s()), "vanka")
 
     def vanka_smooth(self, color=0, omega=1.0, n_inner=1, shift=1.0):
         """One ``vanka_smooth`` launch: adds the face/cell deltas into
@@ -195,10 +195,11 @@ class Grid:
         N.check(self._lib.glide_tile_flags(C.byref(a), self.error_mask.data_ptr(), self._flags.data_ptr(),
                                            self._any_active.data_ptr(), self._s()), "tile flags")
 
-    def vanka_sweep(self, n_iter, n_inner=10, omega=0.5, shift=1.0, step=0.25):
+    def vanka_sweep(self, n_iter, n_inner=10, omega=0.5, shift=1.0, step=0.25, pivot=False):
         """n_iter sweeps with U += omega*delta (glide/grid.py:305-310); ``step``
-        is the local Newton step fraction (reference 0.25)."""
-        self._sweeps(n_iter, n_inner, omega, shift, False, step)
+        is the local Newton step fraction (reference 0.25), ``pivot`` selects
+        row-pivoted local solves."""
+        self._sweeps(n_iter, n_inner, omega, shift, False, step, pivot)
 
     def vanka_sweep_local(self, n_iter, n_inner=10, omega=0.5, shift=1.0, step=0.25):
         """Sweeps gated by error_mask (glide/grid.py:312-317)."""

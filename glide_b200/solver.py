@@ -34,6 +34,7 @@ class SolverSettings:
     smooth_H_correction: bool = False  # bilinear instead of injected coarse H correction
     newton_step: float = 0.25  # fraction of each local Newton step (relaxation_factor, glide/cuda/vanka.cu:416)
     coarse_line_search: bool = False  # finest-level step on the coarse correction (reference: full step)
+    pivoted_lu: bool = False   # row-pivoted local solves (glide/cuda/common.cu:180-233; unused by the reference)
 
     def native(self, thklim) -> N.SolverConfig:
         c = N.SolverConfig()
@@ -46,6 +47,7 @@ class SolverSettings:
         c.smooth_H_correction = int(self.smooth_H_correction)
         c.newton_step = float(self.newton_step)
         c.coarse_line_search = int(self.coarse_line_search)
+        c.pivoted_lu = int(self.pivoted_lu)
         return c
 
 

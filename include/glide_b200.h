@@ -91,12 +91,15 @@ int glide_vanka_sweeps(const GlideLevelArgs* a, const void* f_u, const void* f_v
                        int n_newton, double omega, double shift, const int* flags, const int* any_active,
                        void* scratch, void* stream);
 /* glide_vanka_sweeps with the local Newton step fraction as an argument
- * (0 < newton_step <= 1; the reference fixes it at GLIDE_REF_NEWTON_STEP).
- * Extension, no counterpart in the reference: the tolerance solver's
- * finishing sweeps take full local Newton steps with few iterations. */
+ * (0 < newton_step <= 1; the reference fixes it at GLIDE_REF_NEWTON_STEP) and
+ * pivoted_lu != 0 solving the local systems with row pivoting (the
+ * reference's lu_5x5_solve_pivot, glide/cuda/common.cu:180-233, which its
+ * kernels do not call).  Extension, no counterpart in the reference: the
+ * tolerance solver's finishing sweeps take full local Newton steps with few
+ * iterations. */
 int glide_vanka_sweeps_ex(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
-                          int n_newton, double newton_step, double omega, double shift, const int* flags,
-                          const int* any_active, void* scratch, void* stream);
+                          int n_newton, double newton_step, double omega, double shift, int pivoted_lu,
+                          const int* flags, const int* any_active, void* scratch, void* stream);
 /* Same sweeps as glide_vanka_sweeps for callers that cannot allocate device
  * memory (no counterpart in the reference): the scratch lives in a fixed
  * 10 MiB device array inside the library (glide_noalloc_scratch_bytes()),
@@ -187,6 +190,7 @@ typedef struct GlideSolverConfig {
                                2: no H correction (velocity-only coarse correction) */
     double newton_step;     /* fraction of each local Newton step taken in the forward sweeps;
                                <= 0 means the reference's GLIDE_REF_NEWTON_STEP */
+    int pivoted_lu;         /* 1: local 5x5 systems of the forward sweeps solved with row pivoting */
     int coarse_line_search; /* 1: on the finest level, U = U_pre + a * P(U_c - w_c) with a in
                                {1, 1/2, 1/4, 0} minimising the residual norm (chosen on the
                                device); 0: a = 1 (reference) */

@@ -45,6 +45,48 @@ def lu5_solve(A, b):
     return x
 
 
+def lu5_solve_pivot(A, b, tiny=1e-14):
+    """Row-pivoted LU solve of 5x5 systems, vectorised over cells; restates
+    lu_5x5_solve_pivot (glide/cuda/common.cu:180-233): the largest |entry| of
+    the column is the pivot (first one on ties), a pivot below ``tiny`` skips
+    its elimination step, a diagonal below ``tiny`` in back substitution gives
+    x = 0."""
+    LU = [[np.array(A[i * 5 + j], dtype=float, copy=True) for j in range(5)] for i in range(5)]
+    y = [np.array(b[i], dtype=float, copy=True) for i in range(5)]
+    for k in range(4):
+        p = np.full(LU[k][k].shape, k)
+        best = np.abs(LU[k][k])
+        for i in range(k + 1, 5):
+            a = np.abs(LU[i][k])
+            take = a > best
+            best = np.where(take, a, best)
+            p = np.where(take, i, p)
+        for i in range(k + 1, 5):
+            sw = p == i
+            for j in range(5):
+                LU[k][j], LU[i][j] = np.where(sw, LU[i][j], LU[k][j]), np.where(sw, LU[k][j], LU[i][j])
+            y[k], y[i] = np.where(sw, y[i], y[k]), np.where(sw, y[k], y[i])
+        piv = LU[k][k]
+        live = np.abs(piv) >= tiny
+        safe = np.where(live, piv, 1.0)
+        for i in range(k + 1, 5):
+            f = np.where(live, LU[i][k] / safe, LU[i][k])
+            LU[i][k] = f
+            for j in range(k + 1, 5):
+                LU[i][j] = np.where(live, LU[i][j] - f * LU[k][j], LU[i][j])
+    for i in range(1, 5):
+        for j in range(i):
+            y[i] = y[i] - LU[i][j] * y[j]
+    x = [None] * 5
+    for i in range(4, -1, -1):
+        v = y[i]
+        for j in range(i + 1, 5):
+            v = v - LU[i][j] * x[j]
+        d = LU[i][i]
+        x[i] = np.where(np.abs(d) > tiny, v / np.where(np.abs(d) > tiny, d, 1.0), 0.0)
+    return x
+
+
 class _Frozen:
     """Neighbour values that stay fixed during a cell's local Newton loop."""
 
@@ -245,7 +287,7 @@ def _assemble(fz: _Frozen, ul, ur, vt, vb, Hc, p: Params, dx, dt, with_res, f=No
 
 
 def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt, n_newton=10, cell_on=None,
-                 shift=1.0, return_cells=False, step=0.25):
+                 shift=1.0, return_cells=False, step=0.25, pivot=False):
     """Delta arrays written by one ``vanka_smooth`` launch (vanka.cu:3-439).
 
     Each cell runs ``n_newton`` damped (0.25) Newton steps on its 5 unknowns
@@ -256,7 +298,8 @@ def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt,
     restricts the update to those cells, as the block gating of
     ``vanka_smooth_local`` does.  ``step`` is the Newton step fraction
     (0.25 = relaxation_factor, vanka.cu:416; other values test the
-    extension entry point glide_vanka_sweeps_ex).
+    extension entry point glide_vanka_sweeps_ex); ``pivot`` solves the local
+    systems with ``lu5_solve_pivot``.
     """
     ny, nx = H.shape
     fz = _Frozen(u, v, H, bed, B, beta, p, dx)
@@ -267,7 +310,7 @@ def vanka_deltas(u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, p: Params, dx, dt,
     for _ in range(n_newton):
         Jm, r = _assemble(fz, ul, ur, vt, vb, Hc, p, dx, dt, True, (f_u, f_v, f_H), thklim)
         Jm[0] -= shift; Jm[6] -= shift; Jm[12] -= shift; Jm[18] -= shift; Jm[24] += shift
-        x = lu5_solve(Jm, r)
+        x = lu5_solve_pivot(Jm, r) if pivot else lu5_solve(Jm, r)
         ul = ul - step * x[0]
         ur = ur - step * x[1]
         vt = vt - step * x[2]

@@ -132,18 +132,21 @@ def test_grad_beta(precision, exact):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("shift,step,n_newton", [(1.0, 0.25, 10), (0.0, 0.25, 10), (0.0, 1.0, 2)])
-def test_vanka_sweep(precision, shift, step, n_newton):
+@pytest.mark.parametrize("shift,step,n_newton,pivot", [(1.0, 0.25, 10, False), (0.0, 0.25, 10, False),
+                                                      (0.0, 1.0, 2, False), (0.0, 0.25, 10, True)])
+def test_vanka_sweep(precision, shift, step, n_newton, pivot):
     """One sweep vs the oracle; step 0.25 is the reference smoother, step 1.0
-    with 2 iterations the finishing sweeps of the tolerance solver."""
+    with 2 iterations the finishing sweeps of the tolerance solver, pivot the
+    row-pivoted local solve."""
     from oracle.vanka import vanka_deltas
     st = _state((32, 32), seed=5)
     st["u"] *= 0.02
     st["v"] *= 0.02
     g = _grid(st, precision)
-    g.vanka_sweep(1, n_inner=n_newton, omega=0.5, shift=shift, step=step)
+    g.vanka_sweep(1, n_inner=n_newton, omega=0.5, shift=shift, step=step, pivot=pivot)
     du, dv, dH = vanka_deltas(st["u"], st["v"], st["H"], st["f_u"], st["f_v"], st["f_H"], st["bed"], st["B"],
-                              st["beta"], st["gamma"], _params(), st["dx"], st["dt"], n_newton, shift=shift, step=step)
+                              st["beta"], st["gamma"], _params(), st["dx"], st["dt"], n_newton, shift=shift, step=step,
+                              pivot=pivot)
     tol = TOL[precision] * (1 if precision == "fp64" else 20)
     for a, x0, d in zip((g.u, g.v, g.H), (st["u"], st["v"], st["H"]), (du, dv, dH)):
         assert _rel(_np(a) - x0, 0.5 * d) <= tol

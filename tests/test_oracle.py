@@ -134,3 +134,21 @@ def test_vanka_fixed_point_of_a_solved_local_problem():
     du, dv, dH = vanka_deltas(st["u"], st["v"], st["H"], F[0], F[1], F[2], st["bed"], st["B"], st["beta"],
                               st["gamma"], p, st["dx"], st["dt"], 10)
     assert np.abs(du).max() < 1e-9 and np.abs(dv).max() < 1e-9 and np.abs(dH).max() < 1e-9
+
+
+def test_pivoted_local_solve_matches_dense_solve():
+    """lu5_solve_pivot (the reference's pivoted 5x5 solve) on random systems,
+    one with a zero leading pivot where the unpivoted elimination breaks."""
+    from oracle.vanka import lu5_solve, lu5_solve_pivot
+    rng = np.random.default_rng(12)
+    A = [rng.standard_normal(64) for _ in range(25)]
+    b = [rng.standard_normal(64) for _ in range(5)]
+    A[0][:8] = 0.0
+    M = np.stack(A).reshape(5, 5, 64).transpose(2, 0, 1)
+    ref = np.linalg.solve(M, np.stack(b).T[..., None])[..., 0]
+    x = np.stack(lu5_solve_pivot(A, b)).T
+    good = np.abs(np.linalg.det(M)) > 1e-3
+    assert np.allclose(x[good], ref[good], rtol=1e-8, atol=1e-10)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        xu = np.stack(lu5_solve(A, b)).T
+    assert not np.isfinite(xu[:8]).all()
