@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start (time series) variant")
     ap.add_argument("--no-clocks", action="store_true", help="do not sample nvidia-smi clocks")
+    ap.add_argument("--kernels", action="store_true",
+                    help="per-kernel GB/s table on the marine configuration instead of the metric line")
+    ap.add_argument("--kernels-n", type=int, default=4096, help="grid size of the --kernels table")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying CUDA graphs (for profiler runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -616,10 +619,94 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# algorithmic arrays per cell of one launch (every distinct input read once,
+# every output written once; u and v count as one cell array each)
+KERNEL_ARRAYS = {"residual": 14, "jvp": 13, "vjp": 13, "grad_beta": 8, "vanka_cells": 15, "vanka_sweep": 26,
+                 "norms": 5, "restrict_u": 1.25}
+
+
+def kernel_table(args):
+    """GB/s of every hot kernel on the marine configuration (4096^2 by default;
+    all working sets far exceed the 126 MB L2), FP32 and FP64, CUDA events
+    over 20 launches after a warm-up, against the measured copy bandwidth."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from glide_b200 import _native as N
+    from glide_b200.grid import Grid
+    from glide_b200.kernels import restrict_vfacet
+    from glide_b200.synthetic import marine_case
+    n = args.kernels_n
+    case = marine_case(0, n=n, dx=1000.0 * 4096 / n, n_levels=7)
+    lib = N.load()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    rng = np.random.default_rng(0)
+    table = {}
+    for dtype, tag in ((torch.float32, "fp32"), (torch.float64, "fp64")):
+        g = Grid(n, n, case.dx, dt=DT, dtype=dtype)
+        for k, val in (("H", case.thickness), ("H_prev", case.thickness), ("bed", case.bed), ("B", case.B),
+                       ("beta", case.beta), ("smb", case.smb)):
+            getattr(g, k).copy_(torch.as_tensor(val))
+        g.gamma.fill_(0.1)
+        g.u.copy_(torch.as_tensor(rng.standard_normal((n, n + 1)) * 100.0))
+        g.v.copy_(torch.as_tensor(rng.standard_normal((n + 1, n)) * 100.0))
+        g.f_H.copy_(g.H_prev / DT + g.smb)
+        g.d_U.copy_(torch.as_tensor(rng.standard_normal(g.U.numel())))
+        g.Lambda.copy_(torch.as_tensor(rng.standard_normal(g.U.numel())))
+        grad = torch.empty_like(g.H)
+        coarse = torch.empty((n // 2, n // 2 + 1), dtype=dtype, device="cuda")
+        a = g.level_args()
+        s = torch.cuda.current_stream()
+        saved = g.U.clone()
+        ops = {
+            "residual": lambda: g.compute_residual(),
+            "jvp": lambda: g.compute_jvp(),
+            "vjp": lambda: g.compute_vjp(),
+            "grad_beta": lambda: lib.glide_grad_beta(C.byref(a), g.lambda_u.data_ptr(), g.lambda_v.data_ptr(),
+                                                      grad.data_ptr(), 0, s.cuda_stream),
+            "vanka_cells": lambda: lib.glide_vanka_cells(C.byref(a), g.f_u.data_ptr(), g.f_v.data_ptr(),
+                                                          g.f_H.data_ptr(), 1, 2, 0.0, None, None,
+                                                          g._scratch.data_ptr(), s.cuda_stream),
+            "vanka_sweep": lambda: g.vanka_sweep(1, n_inner=2, omega=0.5, shift=0.0, step=1.0),
+            "norms": lambda: g.residual_norms(),
+            "restrict_u": lambda: restrict_vfacet(g.u, u_coarse=coarse),
+        }
+        esz = 4 if dtype == torch.float32 else 8
+        for name, fn in ops.items():
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(20):
+                fn()
+            e1.record(s)
+            torch.cuda.synchronize()
+            g.U.copy_(saved)
+            t = e0.elapsed_time(e1) / 1e3 / 20
+            gbs = KERNEL_ARRAYS[name] * esz * n * n / t / 1e9
+            table.setdefault(name, {})[tag] = {"us": round(t * 1e6, 1), "GBs": round(gbs, 1),
+                                               "frac": round(gbs / hbm, 3)}
+        del g, saved
+        torch.cuda.empty_cache()
+    print(json.dumps({"kernels": table, "n": n, "case": "marine (floating shelves, beta = 0 there)",
+                      "arrays_per_cell": KERNEL_ARRAYS, "peak_gbs": hbm,
+                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                      "note": "vanka_* are ALU-bound (local 5x5 Newton per cell); GB/s shown for reference"}),
+          flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.kernels:
+        kernel_table(args)
     else:
         run_ours(args)
 
