@@ -232,161 +232,202 @@ __global__ void __launch_bounds__(NTHR) stencil_kernel(
 }
 
 // --------------------------------------------------------------------------
-// residual r = F(U) - f with every input read once (glide/cuda/residuals.cu:
-// 6-292).  Same tile, phases and arithmetic as stencil_kernel<T,false>, but u,
-// v, H, bed and beta of the tile plus the rings the stencil needs are staged
-// into shared memory first with coalesced row loads; the clamped-index rule
-// is applied once while staging (a staged entry at global (i, j) holds the
-// value of the clamped index), so every later read is a plain shared-memory
-// read at unclamped global coordinates.
+// residual, streaming form (what launch_residual runs).  A warp owns a strip
+// of SW = 30 cell columns plus one halo column on each side (lane l holds
+// column j0 - 1 + l) and marches down a chunk of rows.  Everything the
+// stencil needs from the rows above and below stays in registers (u, v for 3
+// rows, H / grounded fraction / surface / beta for 3 cell rows, eta*H for 2,
+// the previous row's syy and vertex sxy); horizontal neighbours come from
+// warp shuffles.  Per row each input field is read once (coalesced), each
+// output written once, and the grounding sigmoid and the surface are computed
+// once per cell instead of once per face.  Loads use clamped rows and
+// per-lane clamped columns, so every in-domain value equals the clamped
+// accessors'; values of out-of-domain cells only enter terms their validity
+// flags zero.  Same arithmetic as stencil_kernel<T,false>.
 // --------------------------------------------------------------------------
-constexpr int RU_R = TY + 4, RU_C = TX + 3;   // u rows [i0-2, i0+TY+2), cols [j0-1, j0+TX+2)
-constexpr int RV_R = TY + 3, RV_C = TX + 4;   // v rows [i0-1, i0+TY+2), cols [j0-2, j0+TX+2)
-constexpr int RC_R = TY + 2, RC_C = TX + 2;   // cells rows [i0-1, i0+TY+1), cols [j0-1, j0+TX+1)
+constexpr int SW = 30;
 
-#ifndef GLIDE_RES_MINB32
-#define GLIDE_RES_MINB32 4
+template <typename T>
+__device__ __forceinline__ T driving_s(T Hm, T Hp, T Sm, T Sp, T dxi, bool valid) {
+    const T w = valid ? T(1) : T(0);
+    const T Havg = T(0.5) * (Hm + Hp);
+    const T dS = Sp - Sm;
+    return Havg * dS * dxi * w;
+}
+
+#ifndef GLIDE_RS_MINB32
+#define GLIDE_RS_MINB32 2
 #endif
-#ifndef GLIDE_RES_MINB64
-#define GLIDE_RES_MINB64 3
+#ifndef GLIDE_RS_MINB64
+#define GLIDE_RS_MINB64 2
 #endif
 template <typename T>
-__global__ void __launch_bounds__(NTHR, sizeof(T) == 4 ? GLIDE_RES_MINB32 : GLIDE_RES_MINB64) residual_kernel(
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_RS_MINB64) residual_stream_kernel(
     T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H,
     const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
-    const T* __restrict__ mask, const T* __restrict__ gamma, Geo g, Phys<T> p) {
-    __shared__ T s_u[RU_R][RU_C];
-    __shared__ T s_v[RV_R][RV_C];
-    __shared__ T s_H[RC_R][RC_C];
-    __shared__ T s_bed[RC_R][RC_C];
-    __shared__ T s_beta[RC_R][RC_C];
-    __shared__ T s_etaH[WR][WC];
-    __shared__ T s_sxx[TY][WC];           // cells rows [i0,i0+TY), cols [j0-1, j0+TX+1)
-    __shared__ T s_syy[WR][TX];           // cells rows [i0-1,i0+TY+1), cols [j0, j0+TX)
-    __shared__ T s_sxy[TY + 1][TX + 1];   // vertices rows [i0, i0+TY], cols [j0, j0+TX]
-
+    const T* __restrict__ mask, const T* __restrict__ gamma, Geo g, Phys<T> p, int n_strips, int rows, int n_warps) {
     const int ny = g.ny, nx = g.nx;
-    const int b = blockIdx.z;
+    const int wid = blockIdx.x * (256 / 32) + threadIdx.x / 32;
+    if (wid >= n_warps) return;  // whole warp
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.y;
     u += b * g.nu(); v += b * g.nv(); H += b * g.nc();
     f_u += b * g.nu(); f_v += b * g.nv(); f_H += b * g.nc();
     bed += b * g.nc(); B += b * g.nc(); beta += b * g.nc(); mask += b * g.nc(); gamma += b * g.nc();
     o_u += b * g.nu(); o_v += b * g.nv(); o_H += b * g.nc();
-    const TileIdx t = tile_idx<TY>();
+
+    const int strip = wid % n_strips, chunk = wid / n_strips;
+    const int i0 = chunk * rows;
+    const int i1 = min(i0 + rows, ny);
+    const int jc = strip * SW - 1 + lane;           // this lane's cell column
+    const int jcc = clampi(jc, 0, nx - 1);          // clamped cell / v column
+    const int juL = clampi(jc, 0, nx);              // this lane's left u-face
+    const int juR = clampi(jc + 1, 0, nx);          // right u-face (own load on lane 31)
+    const int jvL = clampi(jc - 1, 0, nx - 1), jvR = clampi(jc + 1, 0, nx - 1);
+    const bool first = lane == 0, last = lane == 31;
+    const bool own = lane >= 1 && lane <= SW && jc < nx;
+    const unsigned FULL = 0xffffffffu;
     const T dxi = p.dxi;
-    const int ur0 = t.i0 - 2, uc0 = t.j0 - 1, vr0 = t.i0 - 1, vc0 = t.j0 - 2, cr0 = t.i0 - 1, cc0 = t.j0 - 1;
+    const T rr = rho_ratio<T>();
+    auto U = [&](int r, int col) -> T { return __ldg(u + int64_t(clampi(r, 0, ny - 1)) * (nx + 1) + col); };
+    auto Vf = [&](int r, int col) -> T { return __ldg(v + int64_t(clampi(r, 0, ny)) * nx + col); };
+    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + int64_t(clampi(r, 0, ny - 1)) * nx + jcc); };
 
-    stage(&s_u[0][0], u, ny, nx + 1, ur0, uc0, RU_R, RU_C, t.tid, NTHR);
-    stage(&s_v[0][0], v, ny + 1, nx, vr0, vc0, RV_R, RV_C, t.tid, NTHR);
-    stage(&s_H[0][0], H, ny, nx, cr0, cc0, RC_R, RC_C, t.tid, NTHR);
-    stage(&s_bed[0][0], bed, ny, nx, cr0, cc0, RC_R, RC_C, t.tid, NTHR);
-    stage(&s_beta[0][0], beta, ny, nx, cr0, cc0, RC_R, RC_C, t.tid, NTHR);
-    __syncthreads();
-    auto U = [&](int i, int j) -> T { return s_u[i - ur0][j - uc0]; };
-    auto V = [&](int i, int j) -> T { return s_v[i - vr0][j - vc0]; };
+    // state at the start of iteration i: u, v rows i and i+1; cell rows i-1 and i;
+    // eta*H of row i; vertex sxy of row i; syy of row i-1
+    int i = i0 - 2;
+    T uL0 = U(i, juL), uL1 = U(i + 1, juL);
+    T uR0 = last ? U(i, juR) : T(0), uR1 = last ? U(i + 1, juR) : T(0);
+    T v0 = Vf(i, jcc), v1 = Vf(i + 1, jcc);
+    T vL1 = first ? Vf(i + 1, jvL) : T(0), vR1 = last ? Vf(i + 1, jvR) : T(0);
+    T Hm = T(0), gm = T(0), Sm = T(0), bem = T(0);
+    T Hc = T(0), gcc = T(0), Sc = T(0), bec = T(0);
+    T etaH0 = T(0), sxy0 = T(0), syym = T(0);
+    // inputs of iteration k: u, v of row k+2, cell fields of row k+1, the
+    // right-hand side, mask and gamma of output row k.  In FP32 they are
+    // loaded one iteration ahead (software prefetch: two rows of loads in
+    // flight per warp); in FP64 the extra registers would spill.
+    constexpr bool PREFETCH = sizeof(T) == 4;
+    const int jo = jc < nx ? (jc < 0 ? 0 : jc) : nx - 1;  // output column, in range for every lane
+    struct RowIn {
+        T uL2, uR2, v2, vL2, vR2, H, bed, beta, B, fu, fv, fH, m, gam;
+    };
+    auto load_row = [&](int k) {
+        RowIn r;
+        r.uL2 = U(k + 2, juL);
+        r.uR2 = last ? U(k + 2, juR) : T(0);
+        r.v2 = Vf(k + 2, jcc);
+        r.vL2 = first ? Vf(k + 2, jvL) : T(0);
+        r.vR2 = last ? Vf(k + 2, jvR) : T(0);
+        r.H = Cell(H, k + 1); r.bed = Cell(bed, k + 1); r.beta = Cell(beta, k + 1); r.B = Cell(B, k + 1);
+        const int64_t ro = clampi(k, 0, ny - 1);
+        r.fu = __ldg(f_u + ro * (nx + 1) + jo);
+        r.fv = __ldg(f_v + ro * nx + jo);
+        r.fH = __ldg(f_H + ro * nx + jo);
+        r.m = __ldg(mask + ro * nx + jo);
+        r.gam = __ldg(gamma + ro * nx + jo);
+        return r;
+    };
+    RowIn nxt;
+    if constexpr (PREFETCH) nxt = load_row(i);
+    for (; i < i1; ++i) {
+        RowIn cur;
+        if constexpr (PREFETCH) {
+            cur = nxt;
+            nxt = load_row(i + 1);
+        } else {
+            cur = load_row(i);
+        }
+        const T uL2 = cur.uL2, uR2 = cur.uR2, v2 = cur.v2, vL2 = cur.vL2, vR2 = cur.vR2;
+        const T Hp = cur.H, bedp = cur.bed, betap = cur.beta, Bp = cur.B;
+        const T fu_i = cur.fu, fv_i = cur.fv, fH_i = cur.fH, m_i = cur.m, gam_i = cur.gam;
 
-    // phase 1: eta*H on the window (cells clamped into the domain)
-    for (int k = t.tid; k < WR * WC; k += NTHR) {
-        int r = k / WC, c = k - r * WC;
-        int ic = clampi(t.i0 - 1 + r, 0, ny - 1), jc = clampi(t.j0 - 1 + c, 0, nx - 1);
+        T uR0s = __shfl_down_sync(FULL, uL0, 1), uR1s = __shfl_down_sync(FULL, uL1, 1);
+        T uR2s = __shfl_down_sync(FULL, uL2, 1);
+        T vL1s = __shfl_up_sync(FULL, v1, 1), vL2s = __shfl_up_sync(FULL, v2, 1);
+        T vR1s = __shfl_down_sync(FULL, v1, 1), vR2s = __shfl_down_sync(FULL, v2, 1);
+        if (last) { uR0s = uR0; uR1s = uR1; uR2s = uR2; vR1s = vR1; vR2s = vR2; }
+        if (first) { vL1s = vL1; vL2s = vL2; }
+
+        // cell row i+1: grounded fraction, surface, eta*H
+        const T gp = sigmoid(bedp + rr * Hp, p.sig_c);
+        const T Sp = M<T>::max(bedp, -rr * Hp) + Hp;
         EtaIn<T> a;
-        a.ul = U(ic, jc);          a.ur = U(ic, jc + 1);
-        a.vt = V(ic, jc);          a.vb = V(ic + 1, jc);
-        a.u_tl = U(ic - 1, jc);    a.u_tr = U(ic - 1, jc + 1);
-        a.u_bl = U(ic + 1, jc);    a.u_br = U(ic + 1, jc + 1);
-        a.v_lt = V(ic, jc - 1);    a.v_rt = V(ic, jc + 1);
-        a.v_lb = V(ic + 1, jc - 1); a.v_rb = V(ic + 1, jc + 1);
-        EtaOut<T> e = cell_eta(a, __ldg(B + int64_t(ic) * nx + jc), ic, jc, ny, nx, p);
-        s_etaH[r][c] = e.eta * s_H[ic - cr0][jc - cc0];
-    }
-    __syncthreads();
+        a.ul = uL1;   a.ur = uR1s;  a.vt = v1;    a.vb = v2;
+        a.u_tl = uL0; a.u_tr = uR0s; a.u_bl = uL2; a.u_br = uR2s;
+        a.v_lt = vL1s; a.v_rt = vR1s; a.v_lb = vL2s; a.v_rb = vR2s;
+        const T etaHp = cell_eta(a, Bp, clampi(i + 1, 0, ny - 1), jcc, ny, nx, p).eta * Hp;
 
-    // phase 2: normal stresses on cells, shear stresses on vertices
-    for (int k = t.tid; k < TY * WC; k += NTHR) {
-        int r = k / WC, c = k - r * WC;
-        int i = t.i0 + r, j = t.j0 - 1 + c;
-        s_sxx[r][c] = normal_stress<T, true>(U(i, j), U(i, j + 1), V(i, j), V(i + 1, j), s_etaH[r + 1][c], dxi,
-                                             j >= 0 && j < nx).res;
-    }
-    for (int k = t.tid; k < WR * TX; k += NTHR) {
-        int r = k / TX, c = k - r * TX;
-        int i = t.i0 - 1 + r, j = t.j0 + c;
-        s_syy[r][c] = normal_stress<T, false>(U(i, j), U(i, j + 1), V(i, j), V(i + 1, j), s_etaH[r][c + 1], dxi,
-                                              i >= 0 && i < ny).res;
-    }
-    for (int k = t.tid; k < (TY + 1) * (TX + 1); k += NTHR) {
-        int r = k / (TX + 1), c = k - r * (TX + 1);
-        int i = t.i0 + r, j = t.j0 + c;
-        T etaH = T(0.25) * (s_etaH[r][c] + s_etaH[r][c + 1] + s_etaH[r + 1][c] + s_etaH[r + 1][c + 1]);
-        s_sxy[r][c] = shear_stress(U(i - 1, j), U(i, j), V(i, j - 1), V(i, j), etaH, dxi,
-                                   i > 0 && i < ny && j > 0 && j < nx).res;
-    }
-    __syncthreads();
+        // stresses of row i and vertex sxy of row i+1
+        const T sxx = normal_stress<T, true>(uL0, uR0s, v0, v1, etaH0, dxi, jc >= 0 && jc < nx).res;
+        const T syy = normal_stress<T, false>(uL0, uR0s, v0, v1, etaH0, dxi, i >= 0 && i < ny).res;
+        const T etaH0L = __shfl_up_sync(FULL, etaH0, 1), etaHpL = __shfl_up_sync(FULL, etaHp, 1);
+        const T sxy1 = shear_stress(uL0, uL1, vL1s, v1, T(0.25) * (etaH0L + etaH0 + etaHpL + etaHp), dxi,
+                                    i + 1 > 0 && i + 1 < ny && jc > 0 && jc < nx).res;
 
-    // phase 3: owned outputs
-#pragma unroll
-    for (int k = 0; k < RPT; k++) {
-        const int r = t.ty + k * (NTHR / TX);
-        const int c = t.tx;
-        const int i = t.i0 + r, j = t.j0 + c;
-        if (i >= ny || j >= nx) continue;
-        const int sr = r + 1, sc = c + 1;  // this cell in the staged cell windows
-        const T Hc = s_H[sr][sc], Hl = s_H[sr][sc - 1], Hr = s_H[sr][sc + 1];
-        const T Ht = s_H[sr - 1][sc], Hb = s_H[sr + 1][sc];
-        const T bc = s_bed[sr][sc], bl = s_bed[sr][sc - 1], bt = s_bed[sr - 1][sc];
-        const T betac = s_beta[sr][sc], betal = s_beta[sr][sc - 1], betat = s_beta[sr - 1][sc];
-        const T ul = U(i, j), ur = U(i, j + 1), vt = V(i, j), vb = V(i + 1, j);
-        const int64_t ic = int64_t(i) * nx + j;
-
-        // ---- mass row (residuals.cu:50-84)
-        {
-            const T m = mask[ic];
-            Flux<T> ql = upwind_flux(ul, Hl, Hc, j > 0 && j < nx);
-            Flux<T> qr = upwind_flux(ur, Hc, Hr, j + 1 > 0 && j + 1 < nx);
-            Flux<T> qt = upwind_flux(vt, Hc, Ht, i > 0 && i < ny);
-            Flux<T> qb = upwind_flux(vb, Hb, Hc, i + 1 > 0 && i + 1 < ny);
-            Calving<T> cv = calving(Hc, bc, p);
-            T rH = Hc / p.dt - f_H[ic];
-            rH -= cv.res;
-            rH -= ql.res * dxi;
-            rH += qr.res * dxi;
-            rH += qt.res * dxi;
-            rH -= qb.res * dxi;
-            o_H[ic] = (T(1) - m) * rH + m * (Hc - gamma[ic]);
+        if (i >= i0) {  // warp-uniform
+            const T sxxL = __shfl_up_sync(FULL, sxx, 1), sxxR = __shfl_down_sync(FULL, sxx, 1);
+            const T sxy0R = __shfl_down_sync(FULL, sxy0, 1), sxy1R = __shfl_down_sync(FULL, sxy1, 1);
+            const T HcL = __shfl_up_sync(FULL, Hc, 1), HcR = __shfl_down_sync(FULL, Hc, 1);
+            const T gcL = __shfl_up_sync(FULL, gcc, 1), gcR = __shfl_down_sync(FULL, gcc, 1);
+            const T ScL = __shfl_up_sync(FULL, Sc, 1);
+            const T becL = __shfl_up_sync(FULL, bec, 1), becR = __shfl_down_sync(FULL, bec, 1);
+            if (own) {
+                const int64_t ic = int64_t(i) * nx + jc;
+                // ---- mass row (residuals.cu:50-84)
+                {
+                    const T m = m_i;
+                    const Flux<T> ql = upwind_flux(uL0, HcL, Hc, jc > 0 && jc < nx);
+                    const Flux<T> qr = upwind_flux(uR0s, Hc, HcR, jc + 1 > 0 && jc + 1 < nx);
+                    const Flux<T> qt = upwind_flux(v0, Hc, Hm, i > 0 && i < ny);
+                    const Flux<T> qb = upwind_flux(v1, Hp, Hc, i + 1 > 0 && i + 1 < ny);
+                    const Calving<T> cv = calving_g(Hc, gcc, p);
+                    T rH = Hc / p.dt - fH_i;
+                    rH -= cv.res;
+                    rH -= ql.res * dxi;
+                    rH += qr.res * dxi;
+                    rH += qt.res * dxi;
+                    rH -= qb.res * dxi;
+                    o_H[ic] = (T(1) - m) * rH + m * (Hc - gam_i);
+                }
+                // ---- u-face (i, jc) and, at the right edge, (i, nx)
+                {
+                    T val = (sxx - sxxL) * dxi + (sxy0 - sxy1) * dxi;
+                    val += basal_drag_g(uL0, gcL, gcc, becL, bec, p).res -
+                           driving_s(HcL, Hc, ScL, Sc, dxi, jc > 0 && jc < nx);
+                    val -= fu_i;
+                    o_u[int64_t(i) * (nx + 1) + jc] = val;
+                    if (jc == nx - 1) {
+                        T ve = (sxxR - sxx) * dxi + (sxy0R - sxy1R) * dxi;
+                        ve += basal_drag_g(uR0s, gcc, gcR, bec, becR, p).res - T(0) * dxi;
+                        ve -= f_u[int64_t(i) * (nx + 1) + nx];
+                        o_u[int64_t(i) * (nx + 1) + nx] = ve;
+                    }
+                }
+                // ---- v-face (i, jc) and, at the bottom edge, (ny, jc)
+                {
+                    T val = (syym - syy) * dxi + (sxy0R - sxy0) * dxi;
+                    val += basal_drag_g(v0, gm, gcc, bem, bec, p).res -
+                           driving_s(Hc, Hm, Sc, Sm, dxi, i > 0 && i < ny);
+                    val -= fv_i;
+                    o_v[ic] = val;
+                    if (i == ny - 1) {
+                        T ve = (syy - T(0)) * dxi + (sxy1R - sxy1) * dxi;
+                        ve += basal_drag_g(v1, gcc, gp, bec, betap, p).res - T(0) * dxi;
+                        ve -= f_v[int64_t(ny) * nx + jc];
+                        o_v[int64_t(ny) * nx + jc] = ve;
+                    }
+                }
+            }
         }
-        // ---- u-face (i,j) and, at the right edge, (i,nx)
-        for (int e = 0; e < 2; e++) {
-            const int jj = j + e;
-            if (e == 1 && jj != nx) break;
-            const int cc = c + e;
-            T val = (s_sxx[r][cc + 1] - s_sxx[r][cc]) * dxi + (s_sxy[r][cc] - s_sxy[r + 1][cc]) * dxi;
-            const T uf = e ? ur : ul;
-            const T H1 = e ? Hc : Hl, H2 = e ? Hr : Hc;
-            const T b1 = e ? bc : bl, b2 = e ? s_bed[sr][sc + 1] : bc;
-            const T be1 = e ? betac : betal, be2 = e ? s_beta[sr][sc + 1] : betac;
-            BasalDrag<T> tb = basal_drag(uf, H1, H2, b1, b2, be1, be2, p);
-            Driving<T> td = driving(H1, H2, b1, b2, dxi, jj > 0 && jj < nx);
-            val += tb.res - td.res;
-            val -= f_u[int64_t(i) * (nx + 1) + jj];
-            o_u[int64_t(i) * (nx + 1) + jj] = val;
-        }
-        // ---- v-face (i,j) and, at the bottom edge, (ny,j)
-        for (int e = 0; e < 2; e++) {
-            const int ii = i + e;
-            if (e == 1 && ii != ny) break;
-            const int rr = r + e;
-            T val = (s_syy[rr][c] - s_syy[rr + 1][c]) * dxi + (s_sxy[rr][c + 1] - s_sxy[rr][c]) * dxi;
-            const T vf = e ? vb : vt;
-            const T Htop = e ? Hc : Ht, Hbot = e ? Hb : Hc;
-            const T btop = e ? bc : bt, bbot = e ? s_bed[sr + 1][sc] : bc;
-            const T betop = e ? betac : betat, bebot = e ? s_beta[sr + 1][sc] : betac;
-            BasalDrag<T> tb = basal_drag(vf, Htop, Hbot, btop, bbot, betop, bebot, p);
-            Driving<T> td = driving(Hbot, Htop, bbot, btop, dxi, ii > 0 && ii < ny);
-            val += tb.res - td.res;
-            val -= f_v[int64_t(ii) * nx + j];
-            o_v[int64_t(ii) * nx + j] = val;
-        }
+        // roll the window one row down
+        syym = syy; sxy0 = sxy1; etaH0 = etaHp;
+        Hm = Hc; gm = gcc; Sm = Sc; bem = bec;
+        Hc = Hp; gcc = gp; Sc = Sp; bec = betap;
+        uL0 = uL1; uL1 = uL2; uR0 = uR1; uR1 = uR2;
+        v0 = v1; v1 = v2; vL1 = vL2; vR1 = vR2;
     }
 }
 
@@ -644,10 +685,16 @@ int launch_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, c
                     void* r_H, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    glide::count_launch(), residual_kernel<T><<<tile_grid(g), NTHR, 0, s>>>(
+    // streaming residual: strips of SW columns, row chunks sized for ~32 warps per SM
+    const int n_strips = (g.nx + SW - 1) / SW;
+    int rows = int((int64_t(g.ny) * n_strips * g.nb + 148 * 32 - 1) / (148 * 32));
+    rows = rows < 8 ? 8 : (rows > 128 ? 128 : rows);
+    const int n_chunks = (g.ny + rows - 1) / rows;
+    const int n_warps = n_strips * n_chunks;
+    glide::count_launch(), residual_stream_kernel<T><<<dim3((n_warps + 7) / 8, g.nb), 256, 0, s>>>(
         (T*)r_u, (T*)r_v, (T*)r_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
         (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
-        (const T*)a->gamma, g, p);
+        (const T*)a->gamma, g, p, n_strips, rows, n_warps);
     return (int)cudaGetLastError();
 }
 

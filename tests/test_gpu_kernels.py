@@ -59,7 +59,7 @@ def _params(gl=False):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("shape", [(32, 32), (24, 40)])
+@pytest.mark.parametrize("shape", [(32, 32), (24, 40), (33, 47), (70, 100), (5, 3), (130, 61)])
 def test_residual(precision, shape):
     from oracle import ssa
     st = _state(shape)
