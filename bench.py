@@ -181,9 +181,12 @@ def tol_settings():
 
 
 def fast_settings():
-    """Fast path: 2 full local Newton steps per cell, 2 local rounds."""
+    """Fast path: 2 full local Newton steps per cell, 2 local rounds, 6
+    pre/post sweeps, 20 coarsest-level sweeps (the cycle and finishing-sweep
+    counts on the benchmark geometries match those of 10 and 200)."""
     from glide_b200.solver import SolverSettings
-    return SolverSettings(shift=0.0, err_threshold=1e-7, n_local_outer=2, n_newton=2, newton_step=1.0)
+    return SolverSettings(shift=0.0, err_threshold=1e-7, n_local_outer=2, n_newton=2, newton_step=1.0,
+                          n_smooth=6, n_coarse=20)
 
 
 FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0)
