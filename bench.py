@@ -189,7 +189,7 @@ def fast_settings():
                           n_smooth=6, n_coarse=20)
 
 
-FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0)
+FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0, finish_linear="after")
 
 
 def make_cases(n, seeds):
@@ -475,7 +475,8 @@ def run_ours(args):
             "data": "synthetic (seeded grounded-dome geometries, fresh per step)",
             "config": {"workload": f"forward step to {TOL:g} rel. residual, {n}x{n}, dx={DX * 1024 / n:g} m, "
                                    f"{LEVELS} levels, dt={DT:g} a, fresh geometry per step",
-                       "path": "mixed FAS, full-step local Newton x2, FP32/FP64 finishing sweeps + Anderson(3)",
+                       "path": "mixed FAS, full-step local Newton x2, finishing sweeps FP32 (FAS form, then "
+                               "linearised) / FP64 + Anderson(3)",
                        "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas x{world}"},
             **{k: v for k, v in arm(value, info_fast).items() if k not in ("value", "unit")},
             "learned_guess": (arm(guess_val, info_guess) if guess_val is not None else

@@ -83,7 +83,9 @@ class IcePhysics:
         self.finish_fp32 = bool(finish_fp32)
         self.finish_newton = None if finish_newton is None else int(finish_newton)
         self.finish_step = None if finish_step is None else float(finish_step)
-        self.finish_linear = bool(finish_linear)
+        if finish_linear not in (False, True, "after"):
+            raise ValueError('finish_linear must be False, True or "after"')
+        self.finish_linear = finish_linear
         self.finish_patience = int(finish_patience)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
@@ -340,9 +342,10 @@ class IcePhysics:
         correction problem f32 = F32(fl32(U64)) - r64 while they still cut the
         FP64 residual, then FP64 sweeps.  ``finish_anderson`` = m > 0 applies
         Anderson acceleration (depth m) over the blocks to the velocity part.
-        ``finish_linear``: the FP32 blocks solve the linearised correction
-        problem instead (``_linear_block``) and hand over to FP64 after
-        ``finish_patience`` blocks without a new best.  Ten blocks without
+        ``finish_linear``: True -- the FP32 blocks solve the linearised
+        correction problem instead (``_linear_block``) and hand over to FP64
+        after ``finish_patience`` blocks without a new best; "after" -- FAS-form
+        FP32 blocks first, the linearised ones from the FAS form's floor on.  Ten blocks without
         progress restore the best state and continue in FP64 with the
         reference's damped local Newton and no extrapolation; a second
         stagnation ends the finish.
@@ -353,6 +356,8 @@ class IcePhysics:
         rel = hist[-1] if hist else 1.0
         done = 0
         use32 = self.grid32 is not None and self.finish_fp32
+        # FP32 block form: "fas" (correction problem in FAS form), "linear" (linearised correction)
+        form32 = "linear" if self.finish_linear is True else "fas"
         m = self.finish_anderson
         nU = g.nb * (g.nu + g.nv)
         Fs, Gs = [], []
@@ -366,7 +371,8 @@ class IcePhysics:
         while done < max_sweeps and rel > tol:
             x0 = g.U[:nU].clone() if m > 0 else None
             blocks["fp32" if use32 else "fp64"] += 1
-            if use32 and self.finish_linear:
+            if use32 and form32 == "linear":
+                blocks["linear"] = blocks.get("linear", 0) + 1
                 self._linear_block(self.finish_block)
             elif use32:
                 self._fp32_sweeps(self.finish_block, local)
@@ -427,11 +433,18 @@ class IcePhysics:
                 since_best = 0
                 info["finish_safe"] = True
                 continue
-            # the FAS-form FP32 correction floors near eps32 x |operator terms|: hand over to FP64 once a
-            # block gains little; the linear form has no such floor and hands over only when it has not
-            # set a new best for finish_patience blocks (Anderson steps may raise |r| for a while)
-            if use32 and ((self.finish_linear and since_best >= self.finish_patience) or
-                          (not self.finish_linear and rel > 0.7 * prev)):
+            # the FAS-form FP32 correction floors near eps32 x |operator terms|: once a block gains little,
+            # hand over to FP64 -- or, with finish_linear="after", to the linearised FP32 correction, which
+            # has no such floor and is accurate this close to the solution; the linear form hands over to
+            # FP64 when it has not set a new best for finish_patience blocks (Anderson steps may raise |r|)
+            if use32 and form32 == "fas" and rel > 0.7 * prev:
+                if self.finish_linear == "after":
+                    form32 = "linear"
+                    since_best = 0
+                else:
+                    use32 = False
+                Fs, Gs = [], []
+            elif use32 and form32 == "linear" and since_best >= self.finish_patience:
                 use32 = False
                 Fs, Gs = [], []
             prev = rel

@@ -88,17 +88,19 @@ def test_adjoint_fp64_vs_oracle():
     assert _rel(_np(g), og) <= 1e-8
 
 
-def test_mixed_linear_finish_goes_below_the_fp32_correction_floor():
-    """Mixed precision with the linear defect-correction finish reaches
-    |r|/|r0| <= 1e-9 (measured by the FP64 oracle's own residual) with FP32
-    finishing blocks only; the FAS-form FP32 correction floors near eps32
-    times the size of the operator's terms."""
+@pytest.mark.parametrize("mode", [True, "after"])
+def test_mixed_linear_finish_goes_below_the_fp32_correction_floor(mode):
+    """Mixed precision with the linear defect-correction finish (from the
+    start, or after the FAS-form FP32 blocks) reaches |r|/|r0| <= 1e-9
+    (measured by the FP64 oracle's own residual) with FP32 finishing blocks
+    only; the FAS-form FP32 correction floors near eps32 times the size of the
+    operator's terms."""
     from glide_b200 import IcePhysics, SolverSettings
     from oracle.multigrid import OracleIcePhysics, residual_norm
     c = _case(n=64, levels=3)
     st = SolverSettings(shift=0.0, err_threshold=1e-7, n_local_outer=2, n_newton=2, newton_step=1.0)
     ph = IcePhysics(c.ny, c.nx, c.dx, n_levels=c.n_levels, thklim=c.thklim, precision="mixed", settings=st,
-                    finish_fp32=True, finish_linear=True, finish_anderson=3)
+                    finish_fp32=True, finish_linear=mode, finish_anderson=3)
     ph.set_geometry(c.bed, c.thickness)
     ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
     u, v, H = ph.forward(c.dt, tol=1e-9, update_geometry=False, max_vcycles=1)
