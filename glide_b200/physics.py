@@ -54,6 +54,64 @@ def _as_tensor(x, dtype, device, shape=None):
     return t
 
 
+class _Anderson:
+    """Anderson acceleration (depth m) of the velocity over finishing blocks.
+
+    With f_k = G_k - x_k (G_k the state after block k, x_k before it) and
+    dF, dG the differences of consecutive f and G, the next state is
+    G_k - dG gam, gam = argmin |f_k - dF gam| (normal equations, Tikhonov
+    1e-12 trace).  The last m + 1 pairs live in preallocated ring buffers; each
+    block adds one matrix-vector product for the new f's dot products (the
+    small Gram matrix is kept on the host) and one for the combination, so no
+    history is stacked or copied.
+    """
+
+    def __init__(self, m, n, dtype, device):
+        self.m = int(m)
+        self.F = torch.zeros(self.m + 1, n, dtype=dtype, device=device)
+        self.G = torch.zeros(self.m + 1, n, dtype=dtype, device=device)
+        self.gram = np.zeros((self.m + 1, self.m + 1))
+        self.order = []
+
+    def reset(self):
+        self.order = []
+        self.F.zero_()
+        self.G.zero_()
+
+    def step(self, x_before, x):
+        """x (a view of the state) holds the block's result; replace it by the extrapolation."""
+        slot = self.order.pop(0) if len(self.order) == self.m + 1 else len(self.order)
+        if slot in self.order:
+            self.order.remove(slot)
+        self.order.append(slot)
+        torch.sub(x, x_before, out=self.F[slot])
+        self.G[slot].copy_(x)
+        dots = torch.mv(self.F, self.F[slot]).cpu().numpy()
+        self.gram[slot, :] = dots
+        self.gram[:, slot] = dots
+        k = len(self.order)
+        if k < 2:
+            return
+        gf = self.gram[np.ix_(self.order, self.order)]
+        D = np.zeros((k, k - 1))
+        for i in range(k - 1):
+            D[i, i], D[i + 1, i] = -1.0, 1.0
+        Gm = D.T @ gf @ D
+        tr = np.trace(Gm)
+        if not (np.isfinite(tr) and tr > 0):
+            return
+        Gm = Gm + 1e-12 * tr * np.eye(k - 1)
+        try:
+            gam = np.linalg.solve(Gm, D.T @ gf[:, -1])
+        except np.linalg.LinAlgError:
+            return
+        c = -(D @ gam)
+        c[-1] += 1.0
+        full = np.zeros(self.m + 1)
+        full[self.order] = c
+        torch.mv(self.G.T, torch.as_tensor(full, dtype=self.G.dtype, device=self.G.device), out=x)
+
+
 class IcePhysics:
     """GPU shallow-shelf ice-flow model (forward step + adjoint) on one B200."""
 
@@ -360,7 +418,8 @@ class IcePhysics:
         form32 = "linear" if self.finish_linear is True else "fas"
         m = self.finish_anderson
         nU = g.nb * (g.nu + g.nv)
-        Fs, Gs = [], []
+        aa = _Anderson(m, nU, g.dtype, g.device) if m > 0 else None
+        x0 = torch.empty(nU, dtype=g.dtype, device=g.device) if m > 0 else None
         prev = rel
         best, good = rel, self._good_state()
         good.copy_(g.U)
@@ -369,7 +428,8 @@ class IcePhysics:
         blocks = {"fp32": 0, "fp64": 0}
         info["finish_blocks"] = blocks
         while done < max_sweeps and rel > tol:
-            x0 = g.U[:nU].clone() if m > 0 else None
+            if m > 0:
+                x0.copy_(g.U[:nU])
             blocks["fp32" if use32 else "fp64"] += 1
             if use32 and form32 == "linear":
                 blocks["linear"] = blocks.get("linear", 0) + 1
@@ -380,23 +440,9 @@ class IcePhysics:
                 g.vanka_sweep(self.finish_block, omega=st.omega, shift=st.shift, **local)
             done += self.finish_block
             if m > 0:
-                Gx = g.U[:nU].clone()
-                f = Gx - x0
-                Fs.append(f)
-                Gs.append(Gx)
-                if len(Fs) > m + 1:
-                    Fs.pop(0)
-                    Gs.pop(0)
-                if len(Fs) > 1:
-                    dF = torch.stack([Fs[k + 1] - Fs[k] for k in range(len(Fs) - 1)], 1)
-                    dG = torch.stack([Gs[k + 1] - Gs[k] for k in range(len(Gs) - 1)], 1)
-                    # least squares min |f - dF gam| via the (tiny) normal equations; an extrapolation that
-                    # raises |r| is kept on purpose: measured, it shortens the finish (the residual norm
-                    # understates the smooth error it removes)
-                    Gm = dF.T @ dF
-                    Gm = Gm + 1e-12 * torch.trace(Gm) * torch.eye(Gm.shape[0], dtype=Gm.dtype, device=Gm.device)
-                    gam = torch.linalg.solve(Gm, dF.T @ f)
-                    g.U[:nU] = Gx - dG @ gam
+                # an extrapolation that raises |r| is kept on purpose: measured, it shortens the finish
+                # (the residual norm understates the smooth error it removes)
+                aa.step(x0, g.U[:nU])
             rel = self.residual_norm() / r0 if r0 > 0 else 0.0
             hist.append(rel)
             if verbose:
@@ -405,7 +451,8 @@ class IcePhysics:
                 # diverging relaxation: back to the best state, then the reference's damped local Newton
                 g.U.copy_(good)
                 rel = best
-                Fs, Gs = [], []
+                if aa is not None:
+                    aa.reset()
                 safe = dict(n_inner=REFERENCE.n_newton, step=REFERENCE.newton_step)
                 if local == safe:
                     break
@@ -429,7 +476,6 @@ class IcePhysics:
                 g.U.copy_(good)
                 rel = best
                 local, use32, m = safe, False, 0
-                Fs, Gs = [], []
                 since_best = 0
                 info["finish_safe"] = True
                 continue
@@ -443,10 +489,12 @@ class IcePhysics:
                     since_best = 0
                 else:
                     use32 = False
-                Fs, Gs = [], []
+                if aa is not None:
+                    aa.reset()
             elif use32 and form32 == "linear" and since_best >= self.finish_patience:
                 use32 = False
-                Fs, Gs = [], []
+                if aa is not None:
+                    aa.reset()
             prev = rel
         info["finish_sweeps"] = done
         return rel
