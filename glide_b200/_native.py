@@ -24,7 +24,7 @@ SYMBOLS = [
     "glide_adjoint_vcycle", "glide_restrict_parameters", "glide_graph_create", "glide_graph_launch",
     "glide_graph_destroy", "glide_launch_count", "glide_version", "glide_vanka_sweeps_noalloc",
     "glide_noalloc_scratch_bytes", "glide_vanka_sweeps_ex", "glide_vanka_lu", "glide_vanka_linear",
-    "glide_misfit", "glide_tikhonov", "glide_loss_parts",
+    "glide_misfit", "glide_tikhonov", "glide_loss_parts", "glide_jvp_add",
 ]
 
 
@@ -83,6 +83,7 @@ def load():
     sig = {
         "glide_residual": [LA, vp, vp, vp, vp, vp, vp, vp],
         "glide_jvp": [LA, vp, vp, vp, vp, vp, vp, vp],
+        "glide_jvp_add": [LA, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "glide_vjp": [LA, vp, vp, vp, vp, vp, vp, vp, vp, vp, i, vp],
         "glide_grad_beta": [LA, vp, vp, vp, i, vp],
         "glide_vanka_sweeps": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp, vp],

@@ -17,7 +17,9 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_total() { return g_launches.load(std::memory_order_relaxed); }
 
 template <typename T> int launch_residual(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*, cudaStream_t);
-template <typename T> int launch_jvp(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*, cudaStream_t);
+template <typename T>
+int launch_jvp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*,
+               void*, void*, void*, cudaStream_t);
 template <typename T> int launch_vjp(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*, const void*, void*, void*, void*, int, cudaStream_t);
 template <typename T> int launch_grad_beta(const GlideLevelArgs*, const void*, const void*, void*, int, cudaStream_t);
 template <typename T> int launch_vanka_sweeps(const GlideLevelArgs*, const void*, const void*, const void*, int, int, double, double, const int*, const int*, void*, cudaStream_t, double, int);
@@ -82,8 +84,21 @@ int glide_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const v
     int e = check_level(a);
     if (e) return e;
     if (!d_u || !d_v || !d_H || !j_u || !j_v || !j_H) return GLIDE_E_NULL;
-    return TDISPATCH(a->dtype, launch_jvp<float>(a, d_u, d_v, d_H, j_u, j_v, j_H, S(stream)),
-                     launch_jvp<double>(a, d_u, d_v, d_H, j_u, j_v, j_H, S(stream)));
+    return TDISPATCH(a->dtype,
+                     launch_jvp<float>(a, d_u, d_v, d_H, nullptr, nullptr, nullptr, j_u, j_v, j_H, S(stream)),
+                     launch_jvp<double>(a, d_u, d_v, d_H, nullptr, nullptr, nullptr, j_u, j_v, j_H, S(stream)));
+}
+
+int glide_jvp_add(const GlideLevelArgs* a, const void* d_u, const void* d_v, const void* d_H, const void* base_u,
+                  const void* base_v, const void* base_H, void* out_u, void* out_v, void* out_H, void* stream) {
+    int e = check_level(a);
+    if (e) return e;
+    if (!d_u || !d_v || !d_H || !base_u || !base_v || !base_H || !out_u || !out_v || !out_H) return GLIDE_E_NULL;
+    if (out_u == base_u || out_v == base_v || out_H == base_H || out_u == d_u || out_v == d_v || out_H == d_H)
+        return GLIDE_E_SHAPE;
+    return TDISPATCH(a->dtype,
+                     launch_jvp<float>(a, d_u, d_v, d_H, base_u, base_v, base_H, out_u, out_v, out_H, S(stream)),
+                     launch_jvp<double>(a, d_u, d_v, d_H, base_u, base_v, base_H, out_u, out_v, out_H, S(stream)));
 }
 
 int glide_vjp(const GlideLevelArgs* a, const void* l_u, const void* l_v, const void* l_H, const void* f_u,

@@ -1,14 +1,15 @@
 // Residual, JVP, VJP and basal-friction gradient kernels for the SSA system
 // on the MAC staggered grid.
 //
-// Structure (B200): a CTA owns a 32x16 tile of cells with the u-faces on
-// their left, the v-faces on their top (plus the closing face row/column at
-// the domain edge).  Phase 1 computes the cell viscosity (and its tangent) for
-// the tile plus a one-cell ring into shared memory; phase 2 turns it into
-// the cell normal stresses and vertex shear stresses the tile needs; phase 3
-// writes each owned residual entry as a divergence of those stresses plus
-// the face-local drag/driving terms.  Every output has exactly one writer,
-// so results are deterministic (the reference scatters with float atomics,
+// Structure (B200): the residual and the JVP stream -- a warp owns a strip of
+// cell columns and marches down the rows, holding the neighbouring rows in
+// registers and the neighbouring columns in its lanes (warp shuffles), so
+// each input is read once per launch and no shared memory or barrier is
+// needed.  The VJP is tiled: a CTA owns a 32x8 tile of cells, computes the
+// viscosity and its tangent for the tile plus a one-cell ring into shared
+// memory, turns them into the stress tangents the tile needs, and gathers
+// each owned output.  Every output has exactly one writer, so results are
+// deterministic (the reference scatters with float atomics,
 // glide/cuda/residuals.cu:617-1021).
 #include "glide_common.cuh"
 
@@ -32,206 +33,6 @@ template <int TYK> __device__ __forceinline__ TileIdx tile_idx() {
 }
 
 // --------------------------------------------------------------------------
-// residual r = F(U) - f with the active-set row, or the JVP J(U) d
-// (glide/cuda/residuals.cu:6-579)
-// --------------------------------------------------------------------------
-constexpr int TY = 16;                 // residual/JVP tile rows
-constexpr int RPT = TY / (NTHR / TX);  // rows per thread = 2
-constexpr int WR = TY + 2;
-
-template <typename T, bool TAN>
-__global__ void __launch_bounds__(NTHR) stencil_kernel(
-    T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
-    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
-    const T* __restrict__ a_u, const T* __restrict__ a_v, const T* __restrict__ a_H,  // f (residual) or d (JVP)
-    const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
-    const T* __restrict__ mask, const T* __restrict__ gamma, Geo g, Phys<T> p) {
-    __shared__ T s_etaH[WR][WC];
-    __shared__ T s_eta[WR][WC];
-    __shared__ T s_sxx[TY][WC];           // cells rows [i0,i0+TY), cols [j0-1, j0+TX+1)
-    __shared__ T s_syy[WR][TX];           // cells rows [i0-1,i0+TY+1), cols [j0, j0+TX)
-    __shared__ T s_sxy[TY + 1][TX + 1];   // vertices rows [i0, i0+TY], cols [j0, j0+TX]
-    __shared__ T s_detaH[TAN ? WR : 1][TAN ? WC : 1];
-
-    const int ny = g.ny, nx = g.nx;
-    const int b = blockIdx.z;
-    u += b * g.nu(); v += b * g.nv(); H += b * g.nc();
-    a_u += b * g.nu(); a_v += b * g.nv(); a_H += b * g.nc();
-    bed += b * g.nc(); B += b * g.nc(); beta += b * g.nc(); mask += b * g.nc(); gamma += b * g.nc();
-    o_u += b * g.nu(); o_v += b * g.nv(); o_H += b * g.nc();
-    const TileIdx t = tile_idx<TY>();
-    const T dxi = p.dxi;
-
-    // phase 1: eta (and its tangent) on the window
-    for (int k = t.tid; k < WR * WC; k += NTHR) {
-        int r = k / WC, c = k - r * WC;
-        int i = t.i0 - 1 + r, j = t.j0 - 1 + c;
-        int ic = clampi(i, 0, ny - 1), jc = clampi(j, 0, nx - 1);
-        EtaIn<T> ein = eta_inputs(u, v, ic, jc, ny, nx);
-        T Bc = ldc(B, ic, jc, ny, nx);
-        EtaOut<T> e = cell_eta(ein, Bc, ic, jc, ny, nx, p);
-        T Hc = ldc(H, ic, jc, ny, nx);
-        s_eta[r][c] = e.eta;
-        s_etaH[r][c] = e.eta * Hc;
-        if constexpr (TAN) {
-            EtaIn<T> din = eta_inputs(a_u, a_v, ic, jc, ny, nx);
-            T deta = cell_eta_tangent(e, din, Bc, ic, jc, ny, nx, p);
-            s_detaH[r][c] = deta * Hc + e.eta * ldc(a_H, ic, jc, ny, nx);
-        }
-    }
-    __syncthreads();
-
-    // phase 2: normal stresses on cells, shear stresses on vertices
-    // (value for the residual, tangent for the JVP)
-    for (int k = t.tid; k < TY * WC; k += NTHR) {  // sxx
-        int r = k / WC, c = k - r * WC;
-        int i = t.i0 + r, j = t.j0 - 1 + c;
-        T ul = ldu(u, i, j, ny, nx), ur = ldu(u, i, j + 1, ny, nx);
-        T vt = ldv(v, i, j, ny, nx), vb = ldv(v, i + 1, j, ny, nx);
-        NormalStress<T> s = normal_stress<T, true>(ul, ur, vt, vb, s_etaH[r + 1][c], dxi, j >= 0 && j < nx);
-        if constexpr (TAN) {
-            s_sxx[r][c] = s.d_ul * ldu(a_u, i, j, ny, nx) + s.d_ur * ldu(a_u, i, j + 1, ny, nx) +
-                          s.d_vt * ldv(a_v, i, j, ny, nx) + s.d_vb * ldv(a_v, i + 1, j, ny, nx) +
-                          s.d_etaH * s_detaH[r + 1][c];
-        } else {
-            s_sxx[r][c] = s.res;
-        }
-    }
-    for (int k = t.tid; k < WR * TX; k += NTHR) {  // syy
-        int r = k / TX, c = k - r * TX;
-        int i = t.i0 - 1 + r, j = t.j0 + c;
-        T ul = ldu(u, i, j, ny, nx), ur = ldu(u, i, j + 1, ny, nx);
-        T vt = ldv(v, i, j, ny, nx), vb = ldv(v, i + 1, j, ny, nx);
-        NormalStress<T> s = normal_stress<T, false>(ul, ur, vt, vb, s_etaH[r][c + 1], dxi, i >= 0 && i < ny);
-        if constexpr (TAN) {
-            s_syy[r][c] = s.d_ul * ldu(a_u, i, j, ny, nx) + s.d_ur * ldu(a_u, i, j + 1, ny, nx) +
-                          s.d_vt * ldv(a_v, i, j, ny, nx) + s.d_vb * ldv(a_v, i + 1, j, ny, nx) +
-                          s.d_etaH * s_detaH[r][c + 1];
-        } else {
-            s_syy[r][c] = s.res;
-        }
-    }
-    for (int k = t.tid; k < (TY + 1) * (TX + 1); k += NTHR) {  // sxy on vertex (i,j)
-        int r = k / (TX + 1), c = k - r * (TX + 1);
-        int i = t.i0 + r, j = t.j0 + c;
-        // cells around vertex (i,j): (i-1,j-1) (i-1,j) (i,j-1) (i,j) -> window (r,c) (r,c+1) (r+1,c) (r+1,c+1)
-        T etaH = T(0.25) * (s_etaH[r][c] + s_etaH[r][c + 1] + s_etaH[r + 1][c] + s_etaH[r + 1][c + 1]);
-        T ut = ldu(u, i - 1, j, ny, nx), ub = ldu(u, i, j, ny, nx);
-        T vl = ldv(v, i, j - 1, ny, nx), vr = ldv(v, i, j, ny, nx);
-        bool valid = i > 0 && i < ny && j > 0 && j < nx;
-        ShearStress<T> s = shear_stress(ut, ub, vl, vr, etaH, dxi, valid);
-        if constexpr (TAN) {
-            T detaH = T(0.25) * (s_detaH[r][c] + s_detaH[r][c + 1] + s_detaH[r + 1][c] + s_detaH[r + 1][c + 1]);
-            s_sxy[r][c] = s.d_ut * ldu(a_u, i - 1, j, ny, nx) + s.d_ub * ldu(a_u, i, j, ny, nx) +
-                          s.d_vl * ldv(a_v, i, j - 1, ny, nx) + s.d_vr * ldv(a_v, i, j, ny, nx) +
-                          s.d_etaH * detaH;
-        } else {
-            s_sxy[r][c] = s.res;
-        }
-    }
-    __syncthreads();
-
-    // phase 3: owned outputs
-#pragma unroll
-    for (int k = 0; k < RPT; k++) {
-        const int r = t.ty + k * (NTHR / TX);
-        const int c = t.tx;
-        const int i = t.i0 + r, j = t.j0 + c;
-        if (i >= ny || j >= nx) continue;
-        const T Hc = H[int64_t(i) * nx + j];
-        const T Hl = ldc(H, i, j - 1, ny, nx), Hr = ldc(H, i, j + 1, ny, nx);
-        const T Ht = ldc(H, i - 1, j, ny, nx), Hb = ldc(H, i + 1, j, ny, nx);
-        const T bc = bed[int64_t(i) * nx + j];
-        const T bl = ldc(bed, i, j - 1, ny, nx), bt = ldc(bed, i - 1, j, ny, nx);
-        const T betac = beta[int64_t(i) * nx + j];
-        const T betal = ldc(beta, i, j - 1, ny, nx), betat = ldc(beta, i - 1, j, ny, nx);
-        const T ul = u[int64_t(i) * (nx + 1) + j], ur = u[int64_t(i) * (nx + 1) + j + 1];
-        const T vt = v[int64_t(i) * nx + j], vb = v[int64_t(i + 1) * nx + j];
-        T dHc = 0, dHl = 0, dHt = 0, dHr = 0, dHb = 0, dul = 0, dur = 0, dvt = 0, dvb = 0;
-        if constexpr (TAN) {
-            dHc = a_H[int64_t(i) * nx + j];
-            dHl = ldc(a_H, i, j - 1, ny, nx); dHr = ldc(a_H, i, j + 1, ny, nx);
-            dHt = ldc(a_H, i - 1, j, ny, nx); dHb = ldc(a_H, i + 1, j, ny, nx);
-            dul = a_u[int64_t(i) * (nx + 1) + j]; dur = a_u[int64_t(i) * (nx + 1) + j + 1];
-            dvt = a_v[int64_t(i) * nx + j]; dvb = a_v[int64_t(i + 1) * nx + j];
-        }
-
-        // ---- mass row (residuals.cu:50-84)
-        {
-            const T m = mask[int64_t(i) * nx + j];
-            Flux<T> ql = upwind_flux(ul, Hl, Hc, j > 0 && j < nx);
-            Flux<T> qr = upwind_flux(ur, Hc, Hr, j + 1 > 0 && j + 1 < nx);
-            Flux<T> qt = upwind_flux(vt, Hc, Ht, i > 0 && i < ny);         // a = bottom (this cell), b = top
-            Flux<T> qb = upwind_flux(vb, Hb, Hc, i + 1 > 0 && i + 1 < ny);
-            Calving<T> cv = calving(Hc, bc, p);
-            if constexpr (TAN) {
-                T d = dHc / p.dt - cv.d_H * dHc;
-                d -= (ql.d_vel * dul + ql.d_Ha * dHl + ql.d_Hb * dHc) * dxi;
-                d += (qr.d_vel * dur + qr.d_Ha * dHc + qr.d_Hb * dHr) * dxi;
-                d += (qt.d_vel * dvt + qt.d_Ha * dHc + qt.d_Hb * dHt) * dxi;
-                d -= (qb.d_vel * dvb + qb.d_Ha * dHb + qb.d_Hb * dHc) * dxi;
-                o_H[int64_t(i) * nx + j] = (T(1) - m) * d + m * dHc;
-            } else {
-                T rH = Hc / p.dt - a_H[int64_t(i) * nx + j];
-                rH -= cv.res;
-                rH -= ql.res * dxi;
-                rH += qr.res * dxi;
-                rH += qt.res * dxi;
-                rH -= qb.res * dxi;
-                o_H[int64_t(i) * nx + j] = (T(1) - m) * rH + m * (Hc - gamma[int64_t(i) * nx + j]);
-            }
-        }
-
-        // ---- u-face (i,j) and, at the right edge, (i,nx)
-        for (int e = 0; e < 2; e++) {
-            const int jj = j + e;
-            if (e == 1 && jj != nx) break;
-            const int cc = c + e;  // window column offset of cell jj is cc+1 in s_sxx
-            T val = (s_sxx[r][cc + 1] - s_sxx[r][cc]) * dxi + (s_sxy[r][cc] - s_sxy[r + 1][cc]) * dxi;
-            const T uf = e ? ur : ul;
-            const T H1 = e ? Hc : Hl, H2 = e ? Hr : Hc;          // clamped: Hr==Hc at the edge
-            const T b1 = e ? bc : bl, b2 = e ? ldc(bed, i, jj, ny, nx) : bc;
-            const T be1 = e ? betac : betal, be2 = e ? ldc(beta, i, jj, ny, nx) : betac;
-            BasalDrag<T> tb = basal_drag(uf, H1, H2, b1, b2, be1, be2, p);
-            Driving<T> td = driving(H1, H2, b1, b2, dxi, jj > 0 && jj < nx);
-            if constexpr (TAN) {
-                const T duf = e ? dur : dul;
-                const T dH1 = e ? dHc : dHl, dH2 = e ? dHr : dHc;
-                val += tb.d_vel * duf + tb.d_H1 * dH1 + tb.d_H2 * dH2;
-                val -= td.d_Hm * dH1 + td.d_Hp * dH2;
-            } else {
-                val += tb.res - td.res;
-                val -= a_u[int64_t(i) * (nx + 1) + jj];
-            }
-            o_u[int64_t(i) * (nx + 1) + jj] = val;
-        }
-        // ---- v-face (i,j) and, at the bottom edge, (ny,j)
-        for (int e = 0; e < 2; e++) {
-            const int ii = i + e;
-            if (e == 1 && ii != ny) break;
-            const int rr = r + e;  // s_syy row of cell ii-1 is rr, of cell ii is rr+1
-            T val = (s_syy[rr][c] - s_syy[rr + 1][c]) * dxi + (s_sxy[rr][c + 1] - s_sxy[rr][c]) * dxi;
-            const T vf = e ? vb : vt;
-            const T Htop = e ? Hc : Ht, Hbot = e ? Hb : Hc;    // clamped: Hb==Hc at the edge
-            const T btop = e ? bc : bt, bbot = e ? ldc(bed, ii, j, ny, nx) : bc;
-            const T betop = e ? betac : betat, bebot = e ? ldc(beta, ii, j, ny, nx) : betac;
-            BasalDrag<T> tb = basal_drag(vf, Htop, Hbot, btop, bbot, betop, bebot, p);
-            Driving<T> td = driving(Hbot, Htop, bbot, btop, dxi, ii > 0 && ii < ny);
-            if constexpr (TAN) {
-                const T dvf = e ? dvb : dvt;
-                const T dtop = e ? dHc : dHt, dbot = e ? dHb : dHc;
-                val += tb.d_vel * dvf + tb.d_H1 * dtop + tb.d_H2 * dbot;
-                val -= td.d_Hm * dbot + td.d_Hp * dtop;
-            } else {
-                val += tb.res - td.res;
-                val -= a_v[int64_t(ii) * nx + j];
-            }
-            o_v[int64_t(ii) * nx + j] = val;
-        }
-    }
-}
-
-// --------------------------------------------------------------------------
 // residual, streaming form (what launch_residual runs).  A warp owns a strip
 // of SW = 30 cell columns plus one halo column on each side (lane l holds
 // column j0 - 1 + l) and marches down a chunk of rows.  Everything the
@@ -243,7 +44,8 @@ __global__ void __launch_bounds__(NTHR) stencil_kernel(
 // once per cell instead of once per face.  Loads use clamped rows and
 // per-lane clamped columns, so every in-domain value equals the clamped
 // accessors'; values of out-of-domain cells only enter terms their validity
-// flags zero.  Same arithmetic as stencil_kernel<T,false>.
+// flags zero.  Same arithmetic as the reference's residual
+// (glide/cuda/residuals.cu:6-579).
 // --------------------------------------------------------------------------
 constexpr int SW = 30;
 
@@ -428,6 +230,248 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
         Hc = Hp; gcc = gp; Sc = Sp; bec = betap;
         uL0 = uL1; uL1 = uL2; uR0 = uR1; uR1 = uR2;
         v0 = v1; v1 = v2; vL1 = vL2; vR1 = vR2;
+    }
+}
+
+// --------------------------------------------------------------------------
+// JVP J(U) d, streaming form (what launch_jvp runs): the warp-strip march of
+// residual_stream_kernel carrying the direction (d_u, d_v, d_H) beside the
+// state, with the tangent of every term of the residual
+// (glide/cuda/residuals.cu:299-579).  Per cell of row i+1 the
+// kernel forms eta, its tangent and the tangent of eta*H once; per face the
+// drag and driving partials come from the per-cell grounded fraction and the
+// per-cell slope factor dS/dH = 1 + d max(bed, -rho H)/dH.  With ADD the
+// output is base + J d (the linear residual of a defect correction, one pass
+// instead of a JVP and a vector sum).
+// --------------------------------------------------------------------------
+#ifndef GLIDE_JS_MINB32
+#define GLIDE_JS_MINB32 2
+#endif
+#ifndef GLIDE_JS_MINB64
+#define GLIDE_JS_MINB64 1
+#endif
+template <typename T, bool ADD>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_JS_MINB64) jvp_stream_kernel(
+    T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
+    const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
+    const T* __restrict__ d_u, const T* __restrict__ d_v, const T* __restrict__ d_H,
+    const T* __restrict__ base_u, const T* __restrict__ base_v, const T* __restrict__ base_H,
+    const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
+    const T* __restrict__ mask, Geo g, Phys<T> p, int n_strips, int rows, int n_warps) {
+    const int ny = g.ny, nx = g.nx;
+    const int wid = blockIdx.x * (256 / 32) + threadIdx.x / 32;
+    if (wid >= n_warps) return;  // whole warp
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.y;
+    u += b * g.nu(); v += b * g.nv(); H += b * g.nc();
+    d_u += b * g.nu(); d_v += b * g.nv(); d_H += b * g.nc();
+    if constexpr (ADD) { base_u += b * g.nu(); base_v += b * g.nv(); base_H += b * g.nc(); }
+    bed += b * g.nc(); B += b * g.nc(); beta += b * g.nc(); mask += b * g.nc();
+    o_u += b * g.nu(); o_v += b * g.nv(); o_H += b * g.nc();
+
+    const int strip = wid % n_strips, chunk = wid / n_strips;
+    const int i0 = chunk * rows;
+    const int i1 = min(i0 + rows, ny);
+    const int jc = strip * SW - 1 + lane;
+    const int jcc = clampi(jc, 0, nx - 1);
+    const int juL = clampi(jc, 0, nx);
+    const int juR = clampi(jc + 1, 0, nx);
+    const int jvL = clampi(jc - 1, 0, nx - 1), jvR = clampi(jc + 1, 0, nx - 1);
+    const bool first = lane == 0, last = lane == 31;
+    const bool own = lane >= 1 && lane <= SW && jc < nx;
+    const unsigned FULL = 0xffffffffu;
+    const T dxi = p.dxi;
+    const T rr = rho_ratio<T>();
+    auto Uf = [&](const T* a, int r, int col) -> T {
+        return __ldg(a + int64_t(clampi(r, 0, ny - 1)) * (nx + 1) + col);
+    };
+    auto Vf = [&](const T* a, int r, int col) -> T { return __ldg(a + int64_t(clampi(r, 0, ny)) * nx + col); };
+    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + int64_t(clampi(r, 0, ny - 1)) * nx + jcc); };
+    // slope factor of the surface max(bed, -rho H) + H with respect to H
+    auto slope = [&](T Hx, T bx) -> T { return T(1) + (bx > -rr * Hx ? T(0) : -rr); };
+
+    int i = i0 - 2;
+    T uL0 = Uf(u, i, juL), uL1 = Uf(u, i + 1, juL);
+    T uR0 = last ? Uf(u, i, juR) : T(0), uR1 = last ? Uf(u, i + 1, juR) : T(0);
+    T v0 = Vf(v, i, jcc), v1 = Vf(v, i + 1, jcc);
+    T vL1 = first ? Vf(v, i + 1, jvL) : T(0), vR1 = last ? Vf(v, i + 1, jvR) : T(0);
+    T duL0 = Uf(d_u, i, juL), duL1 = Uf(d_u, i + 1, juL);
+    T duR0 = last ? Uf(d_u, i, juR) : T(0), duR1 = last ? Uf(d_u, i + 1, juR) : T(0);
+    T dv0 = Vf(d_v, i, jcc), dv1 = Vf(d_v, i + 1, jcc);
+    T dvL1 = first ? Vf(d_v, i + 1, jvL) : T(0), dvR1 = last ? Vf(d_v, i + 1, jvR) : T(0);
+    T Hm = T(0), gm = T(0), Sm = T(0), bem = T(0), kHm = T(0), dHm = T(0);
+    T Hc = T(0), gcc = T(0), Sc = T(0), bec = T(0), kHc = T(0), dHc = T(0);
+    T etaH0 = T(0), detaH0 = T(0), dsxy0 = T(0), dsyym = T(0);
+    constexpr bool PREFETCH = sizeof(T) == 4;
+    const int jo = jc < nx ? (jc < 0 ? 0 : jc) : nx - 1;
+    struct RowIn {
+        T uL2, uR2, v2, vL2, vR2, duL2, duR2, dv2, dvL2, dvR2, H, bed, beta, B, dH, m, bu, bv, bH;
+    };
+    auto load_row = [&](int k) {
+        RowIn r;
+        r.uL2 = Uf(u, k + 2, juL);
+        r.uR2 = last ? Uf(u, k + 2, juR) : T(0);
+        r.v2 = Vf(v, k + 2, jcc);
+        r.vL2 = first ? Vf(v, k + 2, jvL) : T(0);
+        r.vR2 = last ? Vf(v, k + 2, jvR) : T(0);
+        r.duL2 = Uf(d_u, k + 2, juL);
+        r.duR2 = last ? Uf(d_u, k + 2, juR) : T(0);
+        r.dv2 = Vf(d_v, k + 2, jcc);
+        r.dvL2 = first ? Vf(d_v, k + 2, jvL) : T(0);
+        r.dvR2 = last ? Vf(d_v, k + 2, jvR) : T(0);
+        r.H = Cell(H, k + 1); r.bed = Cell(bed, k + 1); r.beta = Cell(beta, k + 1); r.B = Cell(B, k + 1);
+        r.dH = Cell(d_H, k + 1);
+        const int64_t ro = clampi(k, 0, ny - 1);
+        r.m = __ldg(mask + ro * nx + jo);
+        if constexpr (ADD) {
+            r.bu = __ldg(base_u + ro * (nx + 1) + jo);
+            r.bv = __ldg(base_v + ro * nx + jo);
+            r.bH = __ldg(base_H + ro * nx + jo);
+        } else {
+            r.bu = r.bv = r.bH = T(0);
+        }
+        return r;
+    };
+    RowIn nxt;
+    if constexpr (PREFETCH) nxt = load_row(i);
+    for (; i < i1; ++i) {
+        RowIn cur;
+        if constexpr (PREFETCH) {
+            cur = nxt;
+            nxt = load_row(i + 1);
+        } else {
+            cur = load_row(i);
+        }
+        const T Hp = cur.H, bedp = cur.bed, betap = cur.beta, Bp = cur.B, dHp = cur.dH;
+
+        T uR0s = __shfl_down_sync(FULL, uL0, 1), uR1s = __shfl_down_sync(FULL, uL1, 1);
+        T uR2s = __shfl_down_sync(FULL, cur.uL2, 1);
+        T vL1s = __shfl_up_sync(FULL, v1, 1), vL2s = __shfl_up_sync(FULL, cur.v2, 1);
+        T vR1s = __shfl_down_sync(FULL, v1, 1), vR2s = __shfl_down_sync(FULL, cur.v2, 1);
+        T duR0s = __shfl_down_sync(FULL, duL0, 1), duR1s = __shfl_down_sync(FULL, duL1, 1);
+        T duR2s = __shfl_down_sync(FULL, cur.duL2, 1);
+        T dvL1s = __shfl_up_sync(FULL, dv1, 1), dvL2s = __shfl_up_sync(FULL, cur.dv2, 1);
+        T dvR1s = __shfl_down_sync(FULL, dv1, 1), dvR2s = __shfl_down_sync(FULL, cur.dv2, 1);
+        if (last) {
+            uR0s = uR0; uR1s = uR1; uR2s = cur.uR2; vR1s = vR1; vR2s = cur.vR2;
+            duR0s = duR0; duR1s = duR1; duR2s = cur.duR2; dvR1s = dvR1; dvR2s = cur.dvR2;
+        }
+        if (first) { vL1s = vL1; vL2s = cur.vL2; dvL1s = dvL1; dvL2s = cur.dvL2; }
+
+        // cell row i+1: grounded fraction, surface, slope factor, eta*H and its tangent
+        const T gp = sigmoid(bedp + rr * Hp, p.sig_c);
+        const T Sp = M<T>::max(bedp, -rr * Hp) + Hp;
+        const T kHp = slope(Hp, bedp);
+        T etaHp, detaHp;
+        {
+            EtaIn<T> a, da;
+            a.ul = uL1;   a.ur = uR1s;  a.vt = v1;    a.vb = cur.v2;
+            a.u_tl = uL0; a.u_tr = uR0s; a.u_bl = cur.uL2; a.u_br = uR2s;
+            a.v_lt = vL1s; a.v_rt = vR1s; a.v_lb = vL2s; a.v_rb = vR2s;
+            da.ul = duL1;   da.ur = duR1s;  da.vt = dv1;    da.vb = cur.dv2;
+            da.u_tl = duL0; da.u_tr = duR0s; da.u_bl = cur.duL2; da.u_br = duR2s;
+            da.v_lt = dvL1s; da.v_rt = dvR1s; da.v_lb = dvL2s; da.v_rb = dvR2s;
+            const int ie = clampi(i + 1, 0, ny - 1);
+            const EtaOut<T> e = cell_eta(a, Bp, ie, jcc, ny, nx, p);
+            const T deta = cell_eta_tangent(e, da, Bp, ie, jcc, ny, nx, p);
+            etaHp = e.eta * Hp;
+            detaHp = deta * Hp + e.eta * dHp;
+        }
+
+        // stress tangents of row i and of vertex row i+1
+        T dsxx, dsyy;
+        {
+            const NormalStress<T> s = normal_stress<T, true>(uL0, uR0s, v0, v1, etaH0, dxi, jc >= 0 && jc < nx);
+            dsxx = s.d_ul * duL0 + s.d_ur * duR0s + s.d_vt * dv0 + s.d_vb * dv1 + s.d_etaH * detaH0;
+        }
+        {
+            const NormalStress<T> s = normal_stress<T, false>(uL0, uR0s, v0, v1, etaH0, dxi, i >= 0 && i < ny);
+            dsyy = s.d_ul * duL0 + s.d_ur * duR0s + s.d_vt * dv0 + s.d_vb * dv1 + s.d_etaH * detaH0;
+        }
+        T dsxy1;
+        {
+            const T etaH0L = __shfl_up_sync(FULL, etaH0, 1), etaHpL = __shfl_up_sync(FULL, etaHp, 1);
+            const T detaH0L = __shfl_up_sync(FULL, detaH0, 1), detaHpL = __shfl_up_sync(FULL, detaHp, 1);
+            const ShearStress<T> s = shear_stress(uL0, uL1, vL1s, v1, T(0.25) * (etaH0L + etaH0 + etaHpL + etaHp),
+                                                  dxi, i + 1 > 0 && i + 1 < ny && jc > 0 && jc < nx);
+            const T detaH = T(0.25) * (detaH0L + detaH0 + detaHpL + detaHp);
+            dsxy1 = s.d_ut * duL0 + s.d_ub * duL1 + s.d_vl * dvL1s + s.d_vr * dv1 + s.d_etaH * detaH;
+        }
+
+        if (i >= i0) {  // warp-uniform
+            const T dsxxL = __shfl_up_sync(FULL, dsxx, 1), dsxxR = __shfl_down_sync(FULL, dsxx, 1);
+            const T dsxy0R = __shfl_down_sync(FULL, dsxy0, 1), dsxy1R = __shfl_down_sync(FULL, dsxy1, 1);
+            const T HcL = __shfl_up_sync(FULL, Hc, 1), HcR = __shfl_down_sync(FULL, Hc, 1);
+            const T dHcL = __shfl_up_sync(FULL, dHc, 1), dHcR = __shfl_down_sync(FULL, dHc, 1);
+            const T gcL = __shfl_up_sync(FULL, gcc, 1), gcR = __shfl_down_sync(FULL, gcc, 1);
+            const T ScL = __shfl_up_sync(FULL, Sc, 1), kHcL = __shfl_up_sync(FULL, kHc, 1);
+            const T becL = __shfl_up_sync(FULL, bec, 1), becR = __shfl_down_sync(FULL, bec, 1);
+            if (own) {
+                const int64_t ic = int64_t(i) * nx + jc;
+                // ---- mass row
+                {
+                    const T m = cur.m;
+                    const Flux<T> ql = upwind_flux(uL0, HcL, Hc, jc > 0 && jc < nx);
+                    const Flux<T> qr = upwind_flux(uR0s, Hc, HcR, jc + 1 > 0 && jc + 1 < nx);
+                    const Flux<T> qt = upwind_flux(v0, Hc, Hm, i > 0 && i < ny);
+                    const Flux<T> qb = upwind_flux(v1, Hp, Hc, i + 1 > 0 && i + 1 < ny);
+                    const Calving<T> cv = calving_g(Hc, gcc, p);
+                    T d = dHc / p.dt - cv.d_H * dHc;
+                    d -= (ql.d_vel * duL0 + ql.d_Ha * dHcL + ql.d_Hb * dHc) * dxi;
+                    d += (qr.d_vel * duR0s + qr.d_Ha * dHc + qr.d_Hb * dHcR) * dxi;
+                    d += (qt.d_vel * dv0 + qt.d_Ha * dHc + qt.d_Hb * dHm) * dxi;
+                    d -= (qb.d_vel * dv1 + qb.d_Ha * dHp + qb.d_Hb * dHc) * dxi;
+                    const T jH = (T(1) - m) * d + m * dHc;
+                    o_H[ic] = ADD ? cur.bH + jH : jH;
+                }
+                // ---- u-face (i, jc) and, at the right edge, (i, nx)
+                {
+                    T val = (dsxx - dsxxL) * dxi + (dsxy0 - dsxy1) * dxi;
+                    const BasalDrag<T> tb = basal_drag_g(uL0, gcL, gcc, becL, bec, p);
+                    val += tb.d_vel * duL0 + tb.d_H1 * dHcL + tb.d_H2 * dHc;
+                    const T w = (jc > 0 && jc < nx) ? T(1) : T(0);   // driving: m = left, p = right
+                    const T dS = Sc - ScL, Havg = T(0.5) * (HcL + Hc);
+                    const T d_Hm = (T(0.5) * dS * dxi - Havg * kHcL * dxi) * w;
+                    const T d_Hp = (T(0.5) * dS * dxi + Havg * kHc * dxi) * w;
+                    val -= d_Hm * dHcL + d_Hp * dHc;
+                    o_u[int64_t(i) * (nx + 1) + jc] = ADD ? cur.bu + val : val;
+                    if (jc == nx - 1) {
+                        T ve = (dsxxR - dsxx) * dxi + (dsxy0R - dsxy1R) * dxi;
+                        const BasalDrag<T> te = basal_drag_g(uR0s, gcc, gcR, bec, becR, p);
+                        ve += te.d_vel * duR0s + te.d_H1 * dHc + te.d_H2 * dHcR;
+                        const int64_t oe = int64_t(i) * (nx + 1) + nx;
+                        o_u[oe] = ADD ? __ldg(base_u + oe) + ve : ve;
+                    }
+                }
+                // ---- v-face (i, jc) and, at the bottom edge, (ny, jc)
+                {
+                    T val = (dsyym - dsyy) * dxi + (dsxy0R - dsxy0) * dxi;
+                    const BasalDrag<T> tb = basal_drag_g(v0, gm, gcc, bem, bec, p);
+                    val += tb.d_vel * dv0 + tb.d_H1 * dHm + tb.d_H2 * dHc;
+                    const T w = (i > 0 && i < ny) ? T(1) : T(0);     // driving: m = bottom (row i), p = top
+                    const T dS = Sm - Sc, Havg = T(0.5) * (Hc + Hm);
+                    const T d_Hm = (T(0.5) * dS * dxi - Havg * kHc * dxi) * w;
+                    const T d_Hp = (T(0.5) * dS * dxi + Havg * kHm * dxi) * w;
+                    val -= d_Hm * dHc + d_Hp * dHm;
+                    o_v[ic] = ADD ? cur.bv + val : val;
+                    if (i == ny - 1) {
+                        T ve = (dsyy - T(0)) * dxi + (dsxy1R - dsxy1) * dxi;
+                        const BasalDrag<T> te = basal_drag_g(v1, gcc, gp, bec, betap, p);
+                        ve += te.d_vel * dv1 + te.d_H1 * dHc + te.d_H2 * dHp;
+                        const int64_t oe = int64_t(ny) * nx + jc;
+                        o_v[oe] = ADD ? __ldg(base_v + oe) + ve : ve;
+                    }
+                }
+            }
+        }
+        // roll the window one row down
+        dsyym = dsyy; dsxy0 = dsxy1; etaH0 = etaHp; detaH0 = detaHp;
+        Hm = Hc; gm = gcc; Sm = Sc; bem = bec; kHm = kHc; dHm = dHc;
+        Hc = Hp; gcc = gp; Sc = Sp; bec = betap; kHc = kHp; dHc = dHp;
+        uL0 = uL1; uL1 = cur.uL2; uR0 = uR1; uR1 = cur.uR2;
+        v0 = v1; v1 = cur.v2; vL1 = cur.vL2; vR1 = cur.vR2;
+        duL0 = duL1; duL1 = cur.duL2; duR0 = duR1; duR1 = cur.duR2;
+        dv0 = dv1; dv1 = cur.dv2; dvL1 = cur.dvL2; dvR1 = cur.dvR2;
     }
 }
 
@@ -678,35 +722,53 @@ __global__ void grad_beta_kernel(T* __restrict__ grad, const T* __restrict__ u, 
 // --------------------------------------------------------------------------
 // launchers
 // --------------------------------------------------------------------------
-static inline dim3 tile_grid(const Geo& g, int ty = TY) { return dim3((g.nx + TX - 1) / TX, (g.ny + ty - 1) / ty, g.nb); }
+static inline dim3 tile_grid(const Geo& g, int ty) { return dim3((g.nx + TX - 1) / TX, (g.ny + ty - 1) / ty, g.nb); }
+
+// strips of SW columns, row chunks sized for ~32 warps per SM
+struct StreamShape {
+    int n_strips, rows, n_warps;
+};
+static inline StreamShape stream_shape(const Geo& g) {
+    StreamShape sh;
+    sh.n_strips = (g.nx + SW - 1) / SW;
+    int rows = int((int64_t(g.ny) * sh.n_strips * g.nb + 148 * 32 - 1) / (148 * 32));
+    sh.rows = rows < 8 ? 8 : (rows > 128 ? 128 : rows);
+    sh.n_warps = sh.n_strips * ((g.ny + sh.rows - 1) / sh.rows);
+    return sh;
+}
 
 template <typename T>
 int launch_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, void* r_u, void* r_v,
                     void* r_H, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    // streaming residual: strips of SW columns, row chunks sized for ~32 warps per SM
-    const int n_strips = (g.nx + SW - 1) / SW;
-    int rows = int((int64_t(g.ny) * n_strips * g.nb + 148 * 32 - 1) / (148 * 32));
-    rows = rows < 8 ? 8 : (rows > 128 ? 128 : rows);
-    const int n_chunks = (g.ny + rows - 1) / rows;
-    const int n_warps = n_strips * n_chunks;
-    glide::count_launch(), residual_stream_kernel<T><<<dim3((n_warps + 7) / 8, g.nb), 256, 0, s>>>(
+    const StreamShape sh = stream_shape(g);
+    glide::count_launch(), residual_stream_kernel<T><<<dim3((sh.n_warps + 7) / 8, g.nb), 256, 0, s>>>(
         (T*)r_u, (T*)r_v, (T*)r_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
         (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
-        (const T*)a->gamma, g, p, n_strips, rows, n_warps);
+        (const T*)a->gamma, g, p, sh.n_strips, sh.rows, sh.n_warps);
     return (int)cudaGetLastError();
 }
 
+// j = J(U) d, or j = base + J(U) d when base_u is not null
 template <typename T>
-int launch_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const void* d_H, void* j_u, void* j_v,
-               void* j_H, cudaStream_t s) {
+int launch_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const void* d_H, const void* base_u,
+               const void* base_v, const void* base_H, void* j_u, void* j_v, void* j_H, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    glide::count_launch(), stencil_kernel<T, true><<<tile_grid(g), NTHR, 0, s>>>(
-        (T*)j_u, (T*)j_v, (T*)j_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)d_u, (const T*)d_v,
-        (const T*)d_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
-        (const T*)a->gamma, g, p);
+    const StreamShape sh = stream_shape(g);
+    const dim3 grid((sh.n_warps + 7) / 8, g.nb);
+    if (base_u) {
+        glide::count_launch(), jvp_stream_kernel<T, true><<<grid, 256, 0, s>>>(
+            (T*)j_u, (T*)j_v, (T*)j_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)d_u,
+            (const T*)d_v, (const T*)d_H, (const T*)base_u, (const T*)base_v, (const T*)base_H, (const T*)a->bed,
+            (const T*)a->B, (const T*)a->beta, (const T*)a->mask, g, p, sh.n_strips, sh.rows, sh.n_warps);
+    } else {
+        glide::count_launch(), jvp_stream_kernel<T, false><<<grid, 256, 0, s>>>(
+            (T*)j_u, (T*)j_v, (T*)j_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)d_u,
+            (const T*)d_v, (const T*)d_H, nullptr, nullptr, nullptr, (const T*)a->bed, (const T*)a->B,
+            (const T*)a->beta, (const T*)a->mask, g, p, sh.n_strips, sh.rows, sh.n_warps);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -741,10 +803,10 @@ template int launch_residual<float>(const GlideLevelArgs*, const void*, const vo
                                     cudaStream_t);
 template int launch_residual<double>(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*,
                                      void*, cudaStream_t);
-template int launch_jvp<float>(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*,
-                               cudaStream_t);
-template int launch_jvp<double>(const GlideLevelArgs*, const void*, const void*, const void*, void*, void*, void*,
-                                cudaStream_t);
+template int launch_jvp<float>(const GlideLevelArgs*, const void*, const void*, const void*, const void*,
+                               const void*, const void*, void*, void*, void*, cudaStream_t);
+template int launch_jvp<double>(const GlideLevelArgs*, const void*, const void*, const void*, const void*,
+                                const void*, const void*, void*, void*, void*, cudaStream_t);
 template int launch_vjp<float>(const GlideLevelArgs*, const void*, const void*, const void*, const void*, const void*,
                                const void*, void*, void*, void*, int, cudaStream_t);
 template int launch_vjp<double>(const GlideLevelArgs*, const void*, const void*, const void*, const void*,

@@ -158,6 +158,15 @@ class Grid:
         N.check(self._lib.glide_jvp(C.byref(a), self.d_u.data_ptr(), self.d_v.data_ptr(), self.d_H.data_ptr(),
                                     self.j_u.data_ptr(), self.j_v.data_ptr(), self.j_H.data_ptr(), self._s()), "jvp")
 
+    def jvp_add(self, base, out):
+        """out = base + J(U) d_U in one pass (base, out: monolithic vectors like U)."""
+        bu, bv, bH = self._vec_to_fields(base)
+        ou, ov, oH = self._vec_to_fields(out)
+        a = self.level_args()
+        N.check(self._lib.glide_jvp_add(C.byref(a), self.d_u.data_ptr(), self.d_v.data_ptr(), self.d_H.data_ptr(),
+                                        bu.data_ptr(), bv.data_ptr(), bH.data_ptr(), ou.data_ptr(), ov.data_ptr(),
+                                        oH.data_ptr(), self._s()), "jvp_add")
+
     def compute_vjp(self, exact_boundary=False):
         """l = Lambda^T J(U) (glide/grid.py:240-254)."""
         a = self.level_args()

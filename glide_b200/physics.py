@@ -515,7 +515,7 @@ class IcePhysics:
     def _linear_block(self, n):
         """Defect correction in linear form: r64 = F64(U64) - f64; n FP32
         additive Vanka sweeps for r + J d = 0 linearised at fl32(U64) (local
-        matrices factored once, J d from the FP32 JVP kernel); U64 += fl64(d).
+        matrices factored once, r + J d from one FP32 JVP pass); U64 += fl64(d).
         Unlike the FAS-form correction its rounding error scales with d, not
         with the size of the operator's terms."""
         g64, g32 = self.grid, self.grid32
@@ -537,9 +537,7 @@ class IcePhysics:
             if k == 0:
                 rho = g32.r
             else:
-                g32.compute_jvp()
-                N.check(lib.glide_lincomb(N.F32, g32.z.data_ptr(), g32.r.data_ptr(), 1.0, g32.j.data_ptr(), 1.0,
-                                          ntot, s), "lincomb")
+                g32.jvp_add(g32.r, g32.z)   # rho = r + J d
                 rho = g32.z
             g32.vanka_linear_sweep(rho, g32.d_U, st.omega)
         N.check(lib.glide_convert(N.F64, g64.U.data_ptr(), g32.d_U.data_ptr(), ntot, 1, s), "convert")

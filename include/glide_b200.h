@@ -76,6 +76,12 @@ int glide_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, co
 /* J(U) d. */
 int glide_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const void* d_H, void* j_u, void* j_v,
               void* j_H, void* stream);
+/* out = base + J(U) d in one pass: the linear residual r + J d of a defect
+ * correction.  No counterpart in the reference (its defect correction is
+ * not linearised); same J as glide_jvp.  out must not overlap base or d
+ * (GLIDE_E_SHAPE when a pointer pair is equal). */
+int glide_jvp_add(const GlideLevelArgs* a, const void* d_u, const void* d_v, const void* d_H, const void* base_u,
+                  const void* base_v, const void* base_H, void* out_u, void* out_v, void* out_H, void* stream);
 /* lambda^T J(U); with f_u/f_v/f_H non-null writes f - lambda^T J instead.
  * exact_boundary = 0 reproduces the reference's boundary handling. */
 int glide_vjp(const GlideLevelArgs* a, const void* l_u, const void* l_v, const void* l_H, const void* f_u,

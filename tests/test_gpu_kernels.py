@@ -73,15 +73,63 @@ def test_residual(precision, shape):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("gl", [False, True])
-def test_jvp(precision, gl):
+@pytest.mark.parametrize("shape", [(24, 40), (32, 32), (33, 47), (70, 100), (5, 3), (130, 61)])
+def test_jvp(precision, gl, shape):
     from oracle import ssa
-    st = _state((24, 40), seed=1)
+    st = _state(shape, seed=1)
     g = _grid(st, precision, gl_derivatives=gl)
     g.compute_jvp()
     ref = ssa.jvp(st["u"], st["v"], st["H"], st["d_u"], st["d_v"], st["d_H"], st["bed"], st["B"], st["beta"],
                   st["mask"], st["gamma"], _params(gl), st["dx"], st["dt"])
     for a, b in zip((g.j_u, g.j_v, g.j_H), ref):
         assert _rel(_np(a), b) <= TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [(24, 40), (70, 100), (5, 3)])
+def test_jvp_add(precision, shape):
+    """glide_jvp_add writes base + J d: against the oracle's J d plus base, and
+    within rounding of the base plus the plain JVP's output."""
+    from oracle import ssa
+    st = _state(shape, seed=5)
+    g = _grid(st, precision, gl_derivatives=True)
+    base = torch.randn(g.U.shape, dtype=torch.float64, generator=torch.Generator().manual_seed(3)) * 1e-2
+    base = base.to(g.U.device, g.dtype)
+    out = torch.full_like(g.U, float("nan"))
+    g.jvp_add(base, out)
+    g.compute_jvp()
+    ref = ssa.jvp(st["u"], st["v"], st["H"], st["d_u"], st["d_v"], st["d_H"], st["bed"], st["B"], st["beta"],
+                  st["mask"], st["gamma"], _params(True), st["dx"], st["dt"])
+    ou, ov, oH = g._vec_to_fields(out)
+    bu, bv, bH = g._vec_to_fields(base)
+    for o, b_, j, r in zip((ou, ov, oH), (bu, bv, bH), (g.j_u, g.j_v, g.j_H), ref):
+        assert _rel(_np(o), _np(b_) + r) <= TOL[precision]
+        eps = torch.finfo(g.dtype).eps
+        assert float((o - (b_ + j)).abs().max()) <= 8 * eps * float((b_.abs() + j.abs()).max())
+
+
+def test_jvp_add_rejects_aliasing():
+    import ctypes as C
+    from glide_b200 import _native as N
+    st = _state((24, 40), seed=5)
+    g = _grid(st, "fp32")
+    a = g.level_args()
+    p = [t.data_ptr() for t in (g.d_u, g.d_v, g.d_H, g.r_u, g.r_v, g.r_H)]
+    assert N.load().glide_jvp_add(C.byref(a), *p, p[3], p[4], p[5], N.stream_handle()) == -2
+
+
+def test_jvp_batch_matches_single():
+    """A batch of 3 problems gives the same JVP as 3 single calls."""
+    from glide_b200.grid import Grid
+    sts = [_state((33, 47), seed=s) for s in (20, 21, 22)]
+    g = Grid(33, 47, sts[0]["dx"], dt=10.0, dtype=torch.float32, nb=3, gl_derivatives=True)
+    for k in ("u", "v", "H", "bed", "B", "beta", "mask", "gamma", "d_u", "d_v", "d_H"):
+        getattr(g, k).copy_(torch.as_tensor(np.stack([s[k] for s in sts])))
+    g.compute_jvp()
+    for b, st in enumerate(sts):
+        g1 = _grid(st, "fp32", gl_derivatives=True)
+        g1.compute_jvp()
+        assert torch.equal(g.j_u[b], g1.j_u) and torch.equal(g.j_v[b], g1.j_v) and torch.equal(g.j_H[b], g1.j_H)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
