@@ -449,14 +449,13 @@ class IcePhysics:
                 print(f"  finish {done} sweeps ({'fp32' if use32 else 'fp64'}): |r|/|r0| = {rel:.2e}")
             if not math.isfinite(rel) or rel > 100.0 * best:
                 # diverging relaxation: back to the best state, then the reference's damped local Newton
+                # without extrapolation
                 g.U.copy_(good)
                 rel = best
-                if aa is not None:
-                    aa.reset()
                 safe = dict(n_inner=REFERENCE.n_newton, step=REFERENCE.newton_step)
-                if local == safe:
+                if local == safe and m == 0:
                     break
-                local = safe
+                local, m = safe, 0
                 info["finish_safe"] = True
                 continue
             if rel < best:
