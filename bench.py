@@ -51,7 +51,7 @@ TOL = 1e-6
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N)
@@ -189,7 +189,8 @@ def fast_settings():
                           n_smooth=6, n_coarse=20)
 
 
-FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0, finish_linear="after")
+FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0, finish_linear="after",
+               finish_fas_until=2e-4, finish_fas_patience=8)
 
 
 def make_cases(n, seeds):

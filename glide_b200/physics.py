@@ -119,7 +119,8 @@ class IcePhysics:
                  gl_sigmoid_c=0.1, gl_derivatives=False, *, precision="fp32", device=None,
                  settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0,
                  stall_factor=0.5, finish_block=20, finish_anderson=0, finish_fp32=False, finish_newton=None,
-                 finish_step=None, finish_linear=False, finish_patience=3):
+                 finish_step=None, finish_linear=False, finish_patience=3,
+                 finish_fas_until=math.inf, finish_fas_patience=10):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -145,6 +146,8 @@ class IcePhysics:
             raise ValueError('finish_linear must be False, True or "after"')
         self.finish_linear = finish_linear
         self.finish_patience = int(finish_patience)
+        self.finish_fas_until = float(finish_fas_until)
+        self.finish_fas_patience = int(finish_fas_patience)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
         self.dtype = _PRECISIONS[precision]
@@ -370,7 +373,7 @@ class IcePhysics:
                 break
             prev = rel
         if tol is not None and finish and rel > tol and (stalled or k >= n_max):
-            rel = self._finish(r0, tol, max_finish_sweeps, hist, info, verbose)
+            rel = self._finish(r0, tol, max_finish_sweeps, hist, info, verbose, rel)
         if tol is not None and guess is not None and info["guess_used"] and not rel <= tol:
             # the guess led somewhere the solver cannot finish from: solve again from the plain start
             g.U.copy_(saved)
@@ -393,8 +396,9 @@ class IcePhysics:
                 self.grid32.H_prev.copy_(g.H)
         return g.u, g.v, g.H
 
-    def _finish(self, r0, tol, max_sweeps, hist, info, verbose):
-        """Fine-level Vanka relaxation in blocks until |r|/|r0| <= tol.
+    def _finish(self, r0, tol, max_sweeps, hist, info, verbose, rel):
+        """Fine-level Vanka relaxation in blocks until |r|/|r0| <= tol, from
+        the current state, whose relative residual is ``rel``.
 
         Mixed precision with ``finish_fp32``: blocks of FP32 sweeps on the
         correction problem f32 = F32(fl32(U64)) - r64 while they still cut the
@@ -403,7 +407,15 @@ class IcePhysics:
         ``finish_linear``: True -- the FP32 blocks solve the linearised
         correction problem instead (``_linear_block``) and hand over to FP64
         after ``finish_patience`` blocks without a new best; "after" -- FAS-form
-        FP32 blocks first, the linearised ones from the FAS form's floor on.  Ten blocks without
+        FP32 blocks first, the linearised ones from the FAS form's floor on.
+        A FAS-form block that gains less than 1/0.7 counts as the floor only
+        at |r|/|r0| <= ``finish_fas_until``: above it the gain is small because
+        the smoother is slow, far from the solution, where the linearised
+        correction can diverge (the default, inf, always counts a small gain).
+        The FAS form also ends after ``finish_fas_patience`` blocks without a
+        new best.  For the 1024^2 benchmark geometries, whose FP32 floor lies
+        near 1e-4, 2e-4 and 8 blocks suit both fresh and warm-started steps.
+        Ten blocks without
         progress restore the best state and continue in FP64 with the
         reference's damped local Newton and no extrapolation; a second
         stagnation ends the finish.
@@ -411,7 +423,6 @@ class IcePhysics:
         g = self.grid
         st = self.settings
         g.gamma.fill_(self.thklim)
-        rel = hist[-1] if hist else 1.0
         done = 0
         use32 = self.grid32 is not None and self.finish_fp32
         # FP32 block form: "fas" (correction problem in FAS form), "linear" (linearised correction)
@@ -427,6 +438,7 @@ class IcePhysics:
         local = self._finish_local()
         blocks = {"fp32": 0, "fp64": 0}
         info["finish_blocks"] = blocks
+        fas_until = self.finish_fas_until
         while done < max_sweeps and rel > tol:
             if m > 0:
                 x0.copy_(g.U[:nU])
@@ -478,11 +490,14 @@ class IcePhysics:
                 since_best = 0
                 info["finish_safe"] = True
                 continue
-            # the FAS-form FP32 correction floors near eps32 x |operator terms|: once a block gains little,
+            # the FAS-form FP32 correction floors near eps32 x |operator terms|: once a block gains little
+            # (at |r|/|r0| <= fas_until; above it a small gain means slow smoothing) or none of the last
+            # finish_fas_patience blocks set a new best,
             # hand over to FP64 -- or, with finish_linear="after", to the linearised FP32 correction, which
             # has no such floor and is accurate this close to the solution; the linear form hands over to
             # FP64 when it has not set a new best for finish_patience blocks (Anderson steps may raise |r|)
-            if use32 and form32 == "fas" and rel > 0.7 * prev:
+            if use32 and form32 == "fas" and ((rel > 0.7 * prev and rel <= fas_until) or
+                                              since_best >= self.finish_fas_patience):
                 if self.finish_linear == "after":
                     form32 = "linear"
                     since_best = 0

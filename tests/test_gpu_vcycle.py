@@ -121,13 +121,14 @@ def test_mixed_linear_finish_goes_below_the_fp32_correction_floor(mode):
 def test_fast_path_reaches_tolerance_on_benchmark_geometries():
     """The benchmark's fast path (mixed precision, FAS-form then linearised
     FP32 finishing blocks, Anderson extrapolation, FP64 hand-over) reaches
-    |r|/|r0| <= 1e-6 on seven fresh 1024^2 geometries.  Seed 1 needs the
-    hand-over to FP64 and a divergence recovery; its answer is also checked
+    |r|/|r0| <= 1e-6 on twelve fresh 1024^2 geometries and on a warm-started
+    series.  Seed 9's first V-cycle diverges and is undone; seed 11 needs the
+    FAS form kept through slow, uneven blocks; seed 1's answer is also checked
     with the FP64 oracle's own residual."""
     import torch
     import bench
     from oracle.multigrid import OracleIcePhysics, residual_norm
-    seeds = list(range(7))
+    seeds = list(range(12))
     cases = bench.make_cases(1024, seeds)
     run = bench.Runner(1024, "mixed", settings=bench.fast_settings(), **bench.FAST_KW)
     for seed, case in zip(seeds, cases):
@@ -144,4 +145,12 @@ def test_fast_path_reaches_tolerance_on_benchmark_geometries():
             r0 = residual_norm(g)
             g.u, g.v, g.H = _np(ph.grid.u), _np(ph.grid.v), _np(ph.grid.H)
             assert residual_norm(g) / r0 <= 1.05 * bench.TOL
+    ph = run.ph
+    dev = run.load_device(cases[0])
+    ph.set_geometry(dev["bed"], dev["H"])
+    ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
+    ph.reset_solution()
+    for step in range(6):
+        ph.forward(bench.DT, tol=bench.TOL, max_vcycles=40)
+        assert ph.last_info["rel_residual"] <= bench.TOL, (step, ph.last_info)
     torch.cuda.synchronize()
