@@ -296,8 +296,9 @@ def kernel_timings(runner, launches=20):
 
 
 def roofline(t, n):
-    """Roofline object of the dominant kernel (the FP64 Vanka cell kernel of
-    the finishing sweeps) plus the FP32 cell kernel and the residual stencils."""
+    """Roofline object of the dominant kernel (the FP32 Vanka cell kernel: the
+    V-cycle smoothing and the FP32 finishing blocks, half of the fast path's
+    kernel time) plus the FP64 cell kernel and the residual stencils."""
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -312,21 +313,25 @@ def roofline(t, n):
         return b / sec / 1e9
     fp64_peak = 148 * 64 * 2 * 1.965e9 / 1e12    # DFMA 64/clk/SM (ncu), nominal clock
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
-    t64, t32 = t["cells64"], t.get("cells32")
-    ach = hbm_obj(VANKA_ARRAYS, 8, t64)
-    roof = {"bound": "hbm", "kernel": "vanka_cells_kernel<double> (fine level, finishing sweeps)",
+    t64, t32 = t.get("cells64"), t["cells32"]
+    ach = hbm_obj(VANKA_ARRAYS, 4, t32)
+    roof = {"bound": "hbm", "kernel": "vanka_cells_kernel<float> (fine level, full sweep)",
             "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "peak_source": src,
-            "traffic": VANKA64_DRAM_BYTES_1024 * scale, "traffic_source": "ncu dram__bytes_read+write, one 1024^2 launch",
-            "algorithmic_bytes": ncell * VANKA_ARRAYS * 8, "launch_ms": t64 * 1e3,
-            "limiter": "FP64 issue/latency (ncu: FP64 pipe 33%, 8 warps/SM at 214 registers before the 2-blocks/SM build)",
-            "alu": {"achieved_tflops": ncell * VANKA64_FLOPS_PER_CELL / t64 / 1e12, "peak_tflops": fp64_peak,
-                    "frac": ncell * VANKA64_FLOPS_PER_CELL / t64 / 1e12 / fp64_peak,
-                    "flops_per_cell": VANKA64_FLOPS_PER_CELL, "peak_source": "nominal FP64 (148 SMs x 64 DFMA/clk)"}}
-    if t32:
-        roof["fp32_cells"] = {"kernel": "vanka_cells_kernel<float> (fine level)", "launch_ms": t32 * 1e3,
-                              "achieved_tflops": ncell * VANKA32_FLOPS_PER_CELL / t32 / 1e12,
-                              "frac_fp32_peak": ncell * VANKA32_FLOPS_PER_CELL / t32 / 1e12 / fp32_peak,
-                              "hbm_frac": hbm_obj(VANKA_ARRAYS, 4, t32) / hbm}
+            "traffic": VANKA32_DRAM_BYTES_1024 * scale,
+            "traffic_source": "ncu dram__bytes_read+write, one 1024^2 launch",
+            "algorithmic_bytes": ncell * VANKA_ARRAYS * 4, "launch_ms": t32 * 1e3,
+            "limiter": "FP32 issue/latency (ncu at 1024^2: issue slots 59% active, FMA pipe 34%, ALU 35%, "
+                       "15 warps/SM at 128 registers, 1.4 long-scoreboard stalls per issue)",
+            "alu": {"achieved_tflops": ncell * VANKA32_FLOPS_PER_CELL / t32 / 1e12, "peak_tflops": fp32_peak,
+                    "frac": ncell * VANKA32_FLOPS_PER_CELL / t32 / 1e12 / fp32_peak,
+                    "flops_per_cell": VANKA32_FLOPS_PER_CELL,
+                    "peak_source": "nominal FP32 (148 SMs x 128 FFMA/clk)"}}
+    if t64:
+        roof["fp64_cells"] = {"kernel": "vanka_cells_kernel<double> (fine level, FP64 finishing blocks)",
+                              "launch_ms": t64 * 1e3,
+                              "achieved_tflops": ncell * VANKA64_FLOPS_PER_CELL / t64 / 1e12,
+                              "frac_fp64_peak": ncell * VANKA64_FLOPS_PER_CELL / t64 / 1e12 / fp64_peak,
+                              "hbm_frac": hbm_obj(VANKA_ARRAYS, 8, t64) / hbm}
     roof["stencil"] = {k: {"launch_ms": t[k] * 1e3, "achieved": hbm_obj(RESID_ARRAYS, e, t[k]),
                            "frac": hbm_obj(RESID_ARRAYS, e, t[k]) / hbm}
                        for k, e in (("resid64", 8), ("resid32", 4)) if k in t}
@@ -501,7 +506,7 @@ def run_ours(args):
 # fadd + fmul + 2 ffma per cell), and its DRAM bytes per launch.
 VANKA64_FLOPS_PER_CELL = 1611.0
 VANKA32_FLOPS_PER_CELL = 1324.0
-VANKA64_DRAM_BYTES_1024 = 100.46e6
+VANKA32_DRAM_BYTES_1024 = 46.42e6
 # algorithmic arrays per cell: Vanka reads u, v, H, f_u, f_v, f_H, bed, B,
 # beta, gamma and writes 5 delta arrays; the residual reads 11 and writes 3
 VANKA_ARRAYS = 15
