@@ -594,9 +594,10 @@ def cpu_baseline(case, infos, workers=None):
                                         f"scaled to {case.ny} rows ({t1:.1f} s per sweep) and to a step as above"}}
 
 
-# mean counts of the plain FP64 arm on this workload (GPU run, 3 fresh geometries)
-REF_VCYCLES_PER_STEP = 3.0
-REF_FINISH_SWEEPS_PER_STEP = 313.0
+# mean counts of the plain FP64 arm on this workload (GPU run of the default
+# bench: the 8 timed fresh geometries, seeds 3-10)
+REF_VCYCLES_PER_STEP = 3.125
+REF_FINISH_SWEEPS_PER_STEP = 937.5
 
 
 def run_reference(args):
