@@ -63,7 +63,9 @@ __device__ __forceinline__ T driving_s(T Hm, T Hp, T Sm, T Sp, T dxi, bool valid
 #ifndef GLIDE_RS_MINB64
 #define GLIDE_RS_MINB64 2
 #endif
-template <typename T>
+// Ix: the element-index type of the per-field offsets (int when every field
+// has fewer than 2^31 elements, which keeps the address arithmetic 32-bit).
+template <typename T, typename Ix>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_RS_MINB64) residual_stream_kernel(
     T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
@@ -93,9 +95,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
     const unsigned FULL = 0xffffffffu;
     const T dxi = p.dxi;
     const T rr = rho_ratio<T>();
-    auto U = [&](int r, int col) -> T { return __ldg(u + int64_t(clampi(r, 0, ny - 1)) * (nx + 1) + col); };
-    auto Vf = [&](int r, int col) -> T { return __ldg(v + int64_t(clampi(r, 0, ny)) * nx + col); };
-    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + int64_t(clampi(r, 0, ny - 1)) * nx + jcc); };
+    auto U = [&](int r, int col) -> T { return __ldg(u + Ix(clampi(r, 0, ny - 1)) * (nx + 1) + col); };
+    auto Vf = [&](int r, int col) -> T { return __ldg(v + Ix(clampi(r, 0, ny)) * nx + col); };
+    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + Ix(clampi(r, 0, ny - 1)) * nx + jcc); };
 
     // state at the start of iteration i: u, v rows i and i+1; cell rows i-1 and i;
     // eta*H of row i; vertex sxy of row i; syy of row i-1
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
         r.vL2 = first ? Vf(k + 2, jvL) : T(0);
         r.vR2 = last ? Vf(k + 2, jvR) : T(0);
         r.H = Cell(H, k + 1); r.bed = Cell(bed, k + 1); r.beta = Cell(beta, k + 1); r.B = Cell(B, k + 1);
-        const int64_t ro = clampi(k, 0, ny - 1);
+        const Ix ro = clampi(k, 0, ny - 1);
         r.fu = __ldg(f_u + ro * (nx + 1) + jo);
         r.fv = __ldg(f_v + ro * nx + jo);
         r.fH = __ldg(f_H + ro * nx + jo);
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
             const T ScL = __shfl_up_sync(FULL, Sc, 1);
             const T becL = __shfl_up_sync(FULL, bec, 1), becR = __shfl_down_sync(FULL, bec, 1);
             if (own) {
-                const int64_t ic = int64_t(i) * nx + jc;
+                const Ix ic = Ix(i) * nx + jc;
                 // ---- mass row (residuals.cu:50-84)
                 {
                     const T m = m_i;
@@ -200,12 +202,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
                     val += basal_drag_g(uL0, gcL, gcc, becL, bec, p).res -
                            driving_s(HcL, Hc, ScL, Sc, dxi, jc > 0 && jc < nx);
                     val -= fu_i;
-                    o_u[int64_t(i) * (nx + 1) + jc] = val;
+                    o_u[Ix(i) * (nx + 1) + jc] = val;
                     if (jc == nx - 1) {
                         T ve = (sxxR - sxx) * dxi + (sxy0R - sxy1R) * dxi;
                         ve += basal_drag_g(uR0s, gcc, gcR, bec, becR, p).res - T(0) * dxi;
-                        ve -= f_u[int64_t(i) * (nx + 1) + nx];
-                        o_u[int64_t(i) * (nx + 1) + nx] = ve;
+                        ve -= f_u[Ix(i) * (nx + 1) + nx];
+                        o_u[Ix(i) * (nx + 1) + nx] = ve;
                     }
                 }
                 // ---- v-face (i, jc) and, at the bottom edge, (ny, jc)
@@ -218,8 +220,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
                     if (i == ny - 1) {
                         T ve = (syy - T(0)) * dxi + (sxy1R - sxy1) * dxi;
                         ve += basal_drag_g(v1, gcc, gp, bec, betap, p).res - T(0) * dxi;
-                        ve -= f_v[int64_t(ny) * nx + jc];
-                        o_v[int64_t(ny) * nx + jc] = ve;
+                        ve -= f_v[Ix(ny) * nx + jc];
+                        o_v[Ix(ny) * nx + jc] = ve;
                     }
                 }
             }
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_RS_MINB32 : GLIDE_
 #ifndef GLIDE_JS_MINB64
 #define GLIDE_JS_MINB64 1
 #endif
-template <typename T, bool ADD>
+template <typename T, bool ADD, typename Ix>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_JS_MINB64) jvp_stream_kernel(
     T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
@@ -283,10 +285,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
     const T dxi = p.dxi;
     const T rr = rho_ratio<T>();
     auto Uf = [&](const T* a, int r, int col) -> T {
-        return __ldg(a + int64_t(clampi(r, 0, ny - 1)) * (nx + 1) + col);
+        return __ldg(a + Ix(clampi(r, 0, ny - 1)) * (nx + 1) + col);
     };
-    auto Vf = [&](const T* a, int r, int col) -> T { return __ldg(a + int64_t(clampi(r, 0, ny)) * nx + col); };
-    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + int64_t(clampi(r, 0, ny - 1)) * nx + jcc); };
+    auto Vf = [&](const T* a, int r, int col) -> T { return __ldg(a + Ix(clampi(r, 0, ny)) * nx + col); };
+    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + Ix(clampi(r, 0, ny - 1)) * nx + jcc); };
     // slope factor of the surface max(bed, -rho H) + H with respect to H
     auto slope = [&](T Hx, T bx) -> T { return T(1) + (bx > -rr * Hx ? T(0) : -rr); };
 
@@ -321,7 +323,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
         r.dvR2 = last ? Vf(d_v, k + 2, jvR) : T(0);
         r.H = Cell(H, k + 1); r.bed = Cell(bed, k + 1); r.beta = Cell(beta, k + 1); r.B = Cell(B, k + 1);
         r.dH = Cell(d_H, k + 1);
-        const int64_t ro = clampi(k, 0, ny - 1);
+        const Ix ro = clampi(k, 0, ny - 1);
         r.m = __ldg(mask + ro * nx + jo);
         if constexpr (ADD) {
             r.bu = __ldg(base_u + ro * (nx + 1) + jo);
@@ -407,7 +409,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
             const T ScL = __shfl_up_sync(FULL, Sc, 1), kHcL = __shfl_up_sync(FULL, kHc, 1);
             const T becL = __shfl_up_sync(FULL, bec, 1), becR = __shfl_down_sync(FULL, bec, 1);
             if (own) {
-                const int64_t ic = int64_t(i) * nx + jc;
+                const Ix ic = Ix(i) * nx + jc;
                 // ---- mass row
                 {
                     const T m = cur.m;
@@ -434,12 +436,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
                     const T d_Hm = (T(0.5) * dS * dxi - Havg * kHcL * dxi) * w;
                     const T d_Hp = (T(0.5) * dS * dxi + Havg * kHc * dxi) * w;
                     val -= d_Hm * dHcL + d_Hp * dHc;
-                    o_u[int64_t(i) * (nx + 1) + jc] = ADD ? cur.bu + val : val;
+                    o_u[Ix(i) * (nx + 1) + jc] = ADD ? cur.bu + val : val;
                     if (jc == nx - 1) {
                         T ve = (dsxxR - dsxx) * dxi + (dsxy0R - dsxy1R) * dxi;
                         const BasalDrag<T> te = basal_drag_g(uR0s, gcc, gcR, bec, becR, p);
                         ve += te.d_vel * duR0s + te.d_H1 * dHc + te.d_H2 * dHcR;
-                        const int64_t oe = int64_t(i) * (nx + 1) + nx;
+                        const Ix oe = Ix(i) * (nx + 1) + nx;
                         o_u[oe] = ADD ? __ldg(base_u + oe) + ve : ve;
                     }
                 }
@@ -458,7 +460,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
                         T ve = (dsyy - T(0)) * dxi + (dsxy1R - dsxy1) * dxi;
                         const BasalDrag<T> te = basal_drag_g(v1, gcc, gp, bec, betap, p);
                         ve += te.d_vel * dv1 + te.d_H1 * dHc + te.d_H2 * dHp;
-                        const int64_t oe = int64_t(ny) * nx + jc;
+                        const Ix oe = Ix(ny) * nx + jc;
                         o_v[oe] = ADD ? __ldg(base_v + oe) + ve : ve;
                     }
                 }
@@ -728,6 +730,10 @@ static inline dim3 tile_grid(const Geo& g, int ty) { return dim3((g.nx + TX - 1)
 struct StreamShape {
     int n_strips, rows, n_warps;
 };
+// 32-bit element offsets suffice when every field of one problem has fewer
+// than 2^31 elements (u and v have (ny+1)(nx+1) at most)
+static inline bool index32(const Geo& g) { return int64_t(g.ny + 1) * (g.nx + 1) < (int64_t(1) << 31); }
+
 static inline StreamShape stream_shape(const Geo& g) {
     StreamShape sh;
     sh.n_strips = (g.nx + SW - 1) / SW;
@@ -743,10 +749,17 @@ int launch_residual(const GlideLevelArgs* a, const void* f_u, const void* f_v, c
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     const StreamShape sh = stream_shape(g);
-    glide::count_launch(), residual_stream_kernel<T><<<dim3((sh.n_warps + 7) / 8, g.nb), 256, 0, s>>>(
-        (T*)r_u, (T*)r_v, (T*)r_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u, (const T*)f_v,
-        (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
-        (const T*)a->gamma, g, p, sh.n_strips, sh.rows, sh.n_warps);
+    const dim3 grid((sh.n_warps + 7) / 8, g.nb);
+    auto go = [&](auto kernel) {
+        glide::count_launch(), kernel<<<grid, 256, 0, s>>>(
+            (T*)r_u, (T*)r_v, (T*)r_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_u,
+            (const T*)f_v, (const T*)f_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
+            (const T*)a->gamma, g, p, sh.n_strips, sh.rows, sh.n_warps);
+    };
+    if (index32(g))
+        go(residual_stream_kernel<T, int>);
+    else
+        go(residual_stream_kernel<T, int64_t>);
     return (int)cudaGetLastError();
 }
 
@@ -758,17 +771,17 @@ int launch_jvp(const GlideLevelArgs* a, const void* d_u, const void* d_v, const 
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     const StreamShape sh = stream_shape(g);
     const dim3 grid((sh.n_warps + 7) / 8, g.nb);
-    if (base_u) {
-        glide::count_launch(), jvp_stream_kernel<T, true><<<grid, 256, 0, s>>>(
+    auto go = [&](auto kernel) {
+        glide::count_launch(), kernel<<<grid, 256, 0, s>>>(
             (T*)j_u, (T*)j_v, (T*)j_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)d_u,
             (const T*)d_v, (const T*)d_H, (const T*)base_u, (const T*)base_v, (const T*)base_H, (const T*)a->bed,
             (const T*)a->B, (const T*)a->beta, (const T*)a->mask, g, p, sh.n_strips, sh.rows, sh.n_warps);
-    } else {
-        glide::count_launch(), jvp_stream_kernel<T, false><<<grid, 256, 0, s>>>(
-            (T*)j_u, (T*)j_v, (T*)j_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)d_u,
-            (const T*)d_v, (const T*)d_H, nullptr, nullptr, nullptr, (const T*)a->bed, (const T*)a->B,
-            (const T*)a->beta, (const T*)a->mask, g, p, sh.n_strips, sh.rows, sh.n_warps);
-    }
+    };
+    const bool i32 = index32(g);
+    if (base_u)
+        i32 ? go(jvp_stream_kernel<T, true, int>) : go(jvp_stream_kernel<T, true, int64_t>);
+    else
+        i32 ? go(jvp_stream_kernel<T, false, int>) : go(jvp_stream_kernel<T, false, int64_t>);
     return (int)cudaGetLastError();
 }
 
