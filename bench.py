@@ -67,6 +67,10 @@ def parse():
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying CUDA graphs (for profiler runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--configs", action="store_true",
+                    help="mixed vs FP64 on the 512^2 100-step and the 4096^2 20-step configurations (one JSON line)")
+    ap.add_argument("--configs-only", default=None, help="with --configs: only the configuration named so")
+    ap.add_argument("--configs-steps", type=int, default=0, help="with --configs: steps per series (0: 100 / 20)")
     return ap.parse_args()
 
 
@@ -215,7 +219,7 @@ class Runner:
         d = dict(bed=case.bed, H=case.thickness, B=case.B, beta=case.beta, smb=case.smb)
         return {k: t.as_tensor(v, dtype=self.ph.dtype, device="cuda") for k, v in d.items()}
 
-    def step(self, dev):
+    def step(self, dev, tol=None):
         ph = self.ph
         ph.set_geometry(dev["bed"], dev["H"])
         ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
@@ -223,8 +227,20 @@ class Runner:
         guess = None
         if self.guess_model is not None:
             guess = self.guess_model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"])
-        ph.forward(DT, tol=TOL, max_vcycles=self.max_vcycles, guess=guess)
+        ph.forward(DT, tol=TOL if tol is None else tol, max_vcycles=self.max_vcycles, guess=guess)
         return dict(ph.last_info)
+
+
+def solution_error(sols, refs, n):
+    """Largest relative 2-norm difference per field (u, v, H) between the
+    states in ``sols`` and in ``refs`` (same geometries, same order)."""
+    nu, nv = n * (n + 1), (n + 1) * n
+    out = {"u": 0.0, "v": 0.0, "H": 0.0}
+    for a, b in zip(sols, refs):
+        for name, sl in (("u", slice(0, nu)), ("v", slice(nu, nu + nv)), ("H", slice(nu + nv, None))):
+            d = float((a[sl] - b[sl]).norm() / b[sl].norm().clamp_min(1e-300))
+            out[name] = max(out[name], d)
+    return out
 
 
 def flush_l2(buf):
@@ -236,7 +252,9 @@ def launches(runner):
     return N.load().glide_launch_count() + runner.ph.graph_launches
 
 
-def time_steps(runner, devs, warmup, steps, world, flush):
+def time_steps(runner, devs, warmup, steps, world, flush, keep=None):
+    """W untimed and K timed steps on fresh geometries; with ``keep`` (a list)
+    each timed step's FP64 state is copied there after its timed region."""
     import torch
     infos = []
     for k in range(warmup):
@@ -256,6 +274,8 @@ def time_steps(runner, devs, warmup, steps, world, flush):
         torch.cuda.synchronize()
         runner.launches += launches(runner) - l0
         total += a.elapsed_time(b) / 1e3
+        if keep is not None:
+            keep.append(runner.ph.grid.U.detach().to(torch.float64).clone())
     return total, infos
 
 
@@ -427,7 +447,8 @@ def run_ours(args):
     sampler = ClockSampler(local)
     if not args.no_clocks:
         sampler.start()
-    t_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
+    sol_fast, sol_guess, sol_plain = [], [], []
+    t_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush, sol_fast)
     sampler.stop()
     t_fast = max_over_ranks(t_fast, world)
     value = world * args.steps / t_fast
@@ -436,7 +457,7 @@ def run_ours(args):
     guess_val, info_guess = None, []
     if guess_model is not None and not args.no_guess:
         fast.guess_model = guess_model
-        t_guess, info_guess = time_steps(fast, fdev, args.warmup, args.steps, world, flush)
+        t_guess, info_guess = time_steps(fast, fdev, args.warmup, args.steps, world, flush, sol_guess)
         t_guess = max_over_ranks(t_guess, world)
         guess_val = world * args.steps / t_guess
         fast.guess_model = None
@@ -445,10 +466,30 @@ def run_ours(args):
     if not args.no_plain:
         plain = Runner(n, "fp64", None, args.max_vcycles, use_graphs=not args.eager)
         pdev = [plain.load_device(c) for c in cases]
-        t_plain, info_plain = time_steps(plain, pdev, args.warmup, args.steps, world, flush)
+        t_plain, info_plain = time_steps(plain, pdev, args.warmup, args.steps, world, flush, sol_plain)
         t_plain = max_over_ranks(t_plain, world)
         plain_val = world * args.steps / t_plain
         del plain, pdev
+    # accuracy of the fast path's answers: against the same solve continued to
+    # TOL_TIGHT (its residual is evaluated in FP64, so that state solves the
+    # FP64 discrete equations to TOL_TIGHT, on the same solution branch)
+    sol_tight, rel_tight = [], []
+    for k in range(args.steps):
+        rel_tight.append(fast.step(fdev[args.warmup + k], tol=TOL_TIGHT)["rel_residual"])
+        sol_tight.append(fast.ph.grid.U.detach().to(torch.float64).clone())
+    err = {"fast": solution_error(sol_fast, sol_tight, n),
+           "reference_solution": f"the same solve continued to {TOL_TIGHT:g} relative residual (FP64 residual)",
+           "reference_rel_residual_max": max(rel_tight),
+           "note": "largest relative 2-norm difference per field over the timed steps"}
+    if sol_plain:
+        err["fast_vs_plain_fp64"] = solution_error(sol_fast, sol_plain, n)
+        if sol_guess:
+            err["learned_guess_vs_plain_fp64"] = solution_error(sol_guess, sol_plain, n)
+        err["vs_plain_note"] = ("the implicit step can have more than one solution near floating margins "
+                                "(calving and the grounding sigmoid make the mass balance bistable); the paths "
+                                "may converge to different ones, so these differences do not shrink with the "
+                                "tolerance and are not precision errors")
+    del sol_fast, sol_guess, sol_plain, sol_tight
 
     # end to end through the public API: host (pinned) inputs, H2D each step, D2H of u, v
     e2e_val, h2d, d2h = (None, 0, 0) if args.no_e2e else end_to_end(fast, cases, args, world, flush, n)
@@ -489,6 +530,7 @@ def run_ours(args):
                               {"unavailable": "no trained model" if guess_model is None else "skipped"}),
             "plain_fp64_fas": arm(plain_val, info_plain) if plain_val is not None else None,
             "warm_start": warm,
+            "error_vs_fp64": err,
             "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": fast_launches,
             "roofline": roof,
@@ -596,6 +638,7 @@ def cpu_baseline(case, infos, workers=None):
 
 # mean counts of the plain FP64 arm on this workload (GPU run of the default
 # bench: the 8 timed fresh geometries, seeds 3-10)
+TOL_TIGHT = 1e-8   # tolerance of the reference solutions of the accuracy check
 REF_VCYCLES_PER_STEP = 3.125
 REF_FINISH_SWEEPS_PER_STEP = 937.5
 
@@ -628,6 +671,85 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": workers, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def config_series(case, precision, steps, cot_seed=7):
+    """``steps`` implicit steps of one geometry, each started from the
+    previous one and solved to |r|/|r0| <= TOL (mixed: the fast path; FP64:
+    the plain FAS arm's settings), then the adjoint gradient of a seeded
+    cotangent of (u, v) through the last step, solved to the same relative
+    tolerance.  Returns the final state, the gradient, the time of the steps
+    and the relative residual each step reached."""
+    import torch
+    from glide_b200 import IcePhysics
+    if precision == "mixed":
+        kw = dict(settings=fast_settings(), **FAST_KW)
+    else:
+        kw = dict(settings=tol_settings())
+    ph = IcePhysics(case.ny, case.nx, case.dx, n_levels=case.n_levels, thklim=case.thklim, precision=precision,
+                    **kw, **case.kwargs)
+
+    def start():
+        ph.set_geometry(case.bed, case.thickness)
+        ph.set_parameters(B=case.B, beta=case.beta, smb=case.smb)
+        ph.reset_solution()
+
+    start()
+    ph.forward(case.dt, n_vcycles=1)  # warm-up: builds the per-cycle CUDA graphs
+    start()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rels = []
+    a.record()
+    for _ in range(steps):
+        ph.forward(case.dt, tol=TOL, max_vcycles=40)
+        rels.append(ph.last_info["rel_residual"])
+    b.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    g = ph.grid
+    state = [x.detach().to(torch.float64).clone() for x in (g.u, g.v, g.H)]
+    gen = torch.Generator().manual_seed(cot_seed)
+    cu = torch.randn(tuple(g.u.shape), generator=gen, dtype=torch.float64).to(g.u.device, g.dtype)
+    cv = torch.randn(tuple(g.v.shape), generator=gen, dtype=torch.float64).to(g.u.device, g.dtype)
+    # the adjoint linearises at the last step's state
+    grad = ph.adjoint(cu, cv, torch.zeros_like(g.H), tol=TOL, max_vcycles=40).detach().to(torch.float64).clone()
+    adj_rel = ph.last_adjoint_info.get("rel_residual")
+    del ph
+    torch.cuda.empty_cache()
+    return state, grad, t, rels, adj_rel
+
+
+def run_configs(args):
+    """The 512^2 continental time series and the 4096^2 marine case, the
+    fast mixed-precision path against plain FP64, every step and the final
+    adjoint solved to TOL: throughput and relative difference of the final
+    (u, v, H) and of the adjoint gradient."""
+    from glide_b200.synthetic import ice_sheet_case, marine_case
+
+    def rel(a, b):
+        return float((a - b).norm() / b.norm().clamp_min(1e-300))
+
+    out = {}
+    specs = [("c2_continental_512", ice_sheet_case(0, n=512, dx=1500.0, n_levels=5), args.configs_steps or 100),
+             ("c5_marine_4096", marine_case(0, n=4096, dx=1000.0, n_levels=7), args.configs_steps or 20)]
+    for name, case, steps in specs:
+        if args.configs_only and args.configs_only not in name:
+            continue
+        res = {}
+        for prec in ("mixed", "fp64"):
+            res[prec] = config_series(case, prec, steps)
+        (sm, gm, tm, rm, am), (sd, gd, td, rd, ad) = res["mixed"], res["fp64"]
+        out[name] = {
+            "grid": f"{case.ny}x{case.nx}, dx={case.dx:g} m, {case.n_levels} levels, dt={case.dt:g} a",
+            "steps": steps, "tol": TOL, "series": "each step started from the previous one",
+            "mixed_steps_per_s": steps / tm, "fp64_steps_per_s": steps / td, "speedup": td / tm,
+            "max_rel_residual": {"mixed": max(rm), "fp64": max(rd)},
+            "adjoint_rel_residual": {"mixed": am, "fp64": ad},
+            "rel_diff_vs_fp64": {"u": rel(sm[0], sd[0]), "v": rel(sm[1], sd[1]), "H": rel(sm[2], sd[2]),
+                                 "grad_beta": rel(gm, gd)},
+        }
+    print(json.dumps({"configs": out}), flush=True)
 
 
 # algorithmic arrays per cell of one launch (every distinct input read once,
@@ -718,6 +840,8 @@ def main():
         run_reference(args)
     elif args.kernels:
         kernel_table(args)
+    elif args.configs:
+        run_configs(args)
     else:
         run_ours(args)
 

@@ -586,7 +586,11 @@ class IcePhysics:
         tol |f_adj| (J_m: rows of cells at the thickness limit replaced by the
         identity, as the adjoint smoother sees them); a cycle that cuts the
         residual by less than ``stall_factor`` hands over to fine-level
-        adjoint sweeps.  ``last_adjoint_info`` records the work.
+        adjoint sweeps.  A cycle or block of sweeps whose residual is
+        non-finite or grows 100x over the best one is undone (the best
+        multiplier is kept): a diverging cycle hands over to the sweeps, a
+        diverging block ends the solve.  ``last_adjoint_info`` records the
+        work.
         """
         st = self.settings
         saved_exact = st.exact_adjoint
@@ -603,6 +607,14 @@ class IcePhysics:
             n_max = max_vcycles if tol is not None else n_vcycles
             prev = 1.0
             rel = None
+            # with a tolerance: the best multiplier so far; a cycle or a block of
+            # sweeps whose residual is non-finite or grows 100x is undone
+            best_rel, best = 1.0, None
+            if tol is not None:
+                if getattr(self, "_lam_best", None) is None:
+                    self._lam_best = torch.empty_like(g.Lambda)
+                best = self._lam_best
+                best.zero_()
             for k in range(n_max):
                 if self.precision == "mixed":
                     self._adjoint_dc_step(cfg)
@@ -613,17 +625,33 @@ class IcePhysics:
                 if tol is None:
                     continue
                 rel, f0 = self._adjoint_rel(f0)
+                if not math.isfinite(rel) or rel > 100.0 * best_rel:
+                    g.Lambda.copy_(best)
+                    rel = best_rel
+                    info["cycle_restored"] = True
+                    break
+                if rel < best_rel:
+                    best_rel = rel
+                    best.copy_(g.Lambda)
                 if rel <= tol or rel > self.stall_factor * prev:
                     break
                 prev = rel
             if tol is not None and rel is not None and rel > tol:
                 done = 0
-                while done < max_finish_sweeps and rel > tol and math.isfinite(rel):
+                while done < max_finish_sweeps and rel > tol:
                     g.compute_mask()
                     g.vanka_sweep_adjoint(self.finish_block, omega=st.adj_omega, exact_boundary=exact)
                     g.mask.zero_()
                     done += self.finish_block
                     rel, f0 = self._adjoint_rel(f0)
+                    if not math.isfinite(rel) or rel > 100.0 * best_rel:
+                        g.Lambda.copy_(best)
+                        rel = best_rel
+                        info["finish_restored"] = True
+                        break
+                    if rel < best_rel:
+                        best_rel = rel
+                        best.copy_(g.Lambda)
                 info["finish_sweeps"] = done
             info["rel_residual"] = rel
             self.last_adjoint_info = info

@@ -111,3 +111,47 @@ def test_time_stepped_checkpointed_gradient():
         assert abs(fd2 - fd) <= 1e-4 * abs(fd), "finite differences cross a solution branch"
         ad = (g * d).sum().item()
         assert abs(fd - ad) <= 1e-4 * abs(fd), (k, fd, ad)
+
+
+def test_adjoint_recovers_from_a_diverging_cycle():
+    """Mixed precision adjoint to a tolerance: a cycle that leaves the
+    multiplier non-finite (planted on the host by overwriting it with NaN
+    after the second cycle) is undone, the fine-level sweeps finish from the
+    best multiplier, and the gradient equals the undisturbed solve's to the
+    tolerance's accuracy."""
+    from glide_b200 import IcePhysics, SolverSettings
+    from glide_b200.synthetic import dome_case
+    c = dome_case(0, n=64, dx=5000.0, n_levels=3)
+
+    def physics():
+        ph = IcePhysics(64, 64, c.dx, n_levels=3, thklim=c.thklim, precision="mixed",
+                        settings=SolverSettings(shift=0.0, err_threshold=1e-7))
+        ph.set_geometry(c.bed, c.thickness)
+        ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
+        ph.forward(c.dt, tol=1e-9, update_geometry=False)
+        return ph
+
+    gen = torch.Generator().manual_seed(5)
+    ref = physics()
+    cu = torch.randn(tuple(ref.grid.u.shape), generator=gen, dtype=torch.float64).cuda()
+    cv = torch.randn(tuple(ref.grid.v.shape), generator=gen, dtype=torch.float64).cuda()
+    cH = torch.zeros_like(ref.grid.H)
+    g_ref = ref.adjoint(cu, cv, cH, tol=1e-8).clone()
+    assert ref.last_adjoint_info["rel_residual"] <= 1e-8
+
+    ph = physics()
+    step = ph._adjoint_dc_step
+    calls = []
+
+    def planted(cfg):
+        step(cfg)
+        calls.append(1)
+        if len(calls) == 2:
+            ph.grid.Lambda.fill_(float("nan"))
+    ph._adjoint_dc_step = planted
+    g = ph.adjoint(cu, cv, cH, tol=1e-8)
+    info = ph.last_adjoint_info
+    assert info.get("cycle_restored"), info
+    assert info["rel_residual"] <= 1e-8, info
+    assert torch.isfinite(g).all()
+    assert float((g - g_ref).norm() / g_ref.norm()) <= 1e-6
