@@ -57,6 +57,9 @@ static int check_level(const GlideLevelArgs* a) {
     if (!a) return GLIDE_E_NULL;
     if (a->dtype != GLIDE_F32 && a->dtype != GLIDE_F64) return GLIDE_E_DTYPE;
     if (a->ny < 1 || a->nx < 1 || a->nb < 1) return GLIDE_E_SHAPE;
+    // the stencil and smoother kernels index one problem's fields with 32-bit
+    // element offsets (the largest field, (ny+1)(nx+1), far exceeds HBM first)
+    if (int64_t(a->ny + 1) * (a->nx + 1) >= (int64_t(1) << 31)) return GLIDE_E_TOO_LARGE;
     if (!a->u || !a->v || !a->H || !a->bed || !a->B || !a->beta || !a->mask || !a->gamma) return GLIDE_E_NULL;
     return GLIDE_OK;
 }

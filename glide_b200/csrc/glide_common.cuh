@@ -92,19 +92,21 @@ __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? l
 
 // --------------------------------------------------------------------------
 // clamped global accessors (same semantics as glide/cuda/common.cu:78-125:
-// every index is clamped to the field's own extent)
+// every index is clamped to the field's own extent).  Offsets are 32-bit
+// element counts: the entry points reject problems whose fields reach 2^31
+// elements (GLIDE_E_TOO_LARGE).
 // --------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T ldu(const T* __restrict__ u, int i, int j, int ny, int nx) {
-    return __ldg(u + int64_t(clampi(i, 0, ny - 1)) * (nx + 1) + clampi(j, 0, nx));
+    return __ldg(u + (clampi(i, 0, ny - 1) * (nx + 1) + clampi(j, 0, nx)));
 }
 template <typename T>
 __device__ __forceinline__ T ldv(const T* __restrict__ v, int i, int j, int ny, int nx) {
-    return __ldg(v + int64_t(clampi(i, 0, ny)) * nx + clampi(j, 0, nx - 1));
+    return __ldg(v + (clampi(i, 0, ny) * nx + clampi(j, 0, nx - 1)));
 }
 template <typename T>
 __device__ __forceinline__ T ldc(const T* __restrict__ a, int i, int j, int ny, int nx) {
-    return __ldg(a + int64_t(clampi(i, 0, ny - 1)) * nx + clampi(j, 0, nx - 1));
+    return __ldg(a + (clampi(i, 0, ny - 1) * nx + clampi(j, 0, nx - 1)));
 }
 
 // Stage a clamped window [r0, r0+R) x [c0, c0+C) of a (rows x cols) field

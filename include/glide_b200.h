@@ -45,7 +45,7 @@ extern "C" {
 #define GLIDE_E_SHAPE (-2)
 #define GLIDE_E_NULL (-3)
 #define GLIDE_E_GRAPH (-4)
-#define GLIDE_E_TOO_LARGE (-5)
+#define GLIDE_E_TOO_LARGE (-5)  /* a field of one problem reaches 2^31 elements, or a fixed buffer is too small */
 
 /* Fraction of each local Newton step the reference's Vanka smoother takes
  * (relaxation_factor, glide/cuda/vanka.cu:416). */
