@@ -507,13 +507,15 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BL
         load_patch(P, s_eta, r, c, u, v, H, bed, beta, i, j, ny, nx, p);
         make_frozen(F, P, ny, nx, p);
     }
-    const T ul0 = u[int64_t(i) * (nx + 1) + j], ur0 = u[int64_t(i) * (nx + 1) + j + 1];
-    const T vt0 = v[int64_t(i) * nx + j], vb0 = v[int64_t(i + 1) * nx + j];
-    const T H0 = H[int64_t(i) * nx + j];
-    const T fu_l = f_u[int64_t(i) * (nx + 1) + j], fu_r = f_u[int64_t(i) * (nx + 1) + j + 1];
-    const T fv_t = f_v[int64_t(i) * nx + j], fv_b = f_v[int64_t(i + 1) * nx + j];
-    const T fH = f_H[int64_t(i) * nx + j];
-    const T thk = gamma[int64_t(i) * nx + j];
+    // 32-bit offsets within one field (the entry points bound a field below 2^31 elements)
+    const int iu = i * (nx + 1) + j, ic32 = i * nx + j;
+    const T ul0 = u[iu], ur0 = u[iu + 1];
+    const T vt0 = v[ic32], vb0 = v[ic32 + nx];
+    const T H0 = H[ic32];
+    const T fu_l = f_u[iu], fu_r = f_u[iu + 1];
+    const T fv_t = f_v[ic32], fv_b = f_v[ic32 + nx];
+    const T fH = f_H[ic32];
+    const T thk = gamma[ic32];
     const T dti = T(1) / p.dt;
     T ul = ul0, ur = ur0, vt = vt0, vb = vb0, Hc = H0;
     for (int it = 0; it < n_newton; it++) {
