@@ -14,7 +14,8 @@ _LIB_PATH = Path(__file__).resolve().parent / "libglide_b200.so"
 _lib = None
 
 F32, F64 = 0, 1
-ERRORS = {-1: "unsupported dtype", -2: "bad shape or argument", -3: "null pointer", -4: "CUDA graph failure"}
+ERRORS = {-1: "unsupported dtype", -2: "bad shape or argument", -3: "null pointer", -4: "CUDA graph failure",
+          -5: "too large (a field of 2^31 elements or more, or a fixed buffer too small)"}
 
 SYMBOLS = [
     "glide_residual", "glide_jvp", "glide_vjp", "glide_grad_beta", "glide_vanka_sweeps", "glide_vanka_cells",

@@ -51,3 +51,6 @@ def test_argument_validation_without_gpu():
     assert lib.glide_residual(C.byref(a), None, None, None, None, None, None, None) == -2   # shape
     assert lib.glide_restrict(5, 0, 0, None, None, 4, 4, 1, None) == -1
     assert lib.glide_fascd_vcycle(None, 0, 0, 1, None, None) == -3
+    # a problem whose fields reach 2^31 elements is refused before any launch
+    a.ny, a.nx = 50_000, 50_000
+    assert lib.glide_residual(C.byref(a), None, None, None, None, None, None, None) == -5   # too large
