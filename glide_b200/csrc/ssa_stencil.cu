@@ -1,36 +1,16 @@
 // Residual, JVP, VJP and basal-friction gradient kernels for the SSA system
 // on the MAC staggered grid.
 //
-// Structure (B200): the residual and the JVP stream -- a warp owns a strip of
-// cell columns and marches down the rows, holding the neighbouring rows in
-// registers and the neighbouring columns in its lanes (warp shuffles), so
-// each input is read once per launch and no shared memory or barrier is
-// needed.  The VJP is tiled: a CTA owns a 32x8 tile of cells, computes the
-// viscosity and its tangent for the tile plus a one-cell ring into shared
-// memory, turns them into the stress tangents the tile needs, and gathers
-// each owned output.  Every output has exactly one writer, so results are
-// deterministic (the reference scatters with float atomics,
+// Structure (B200): the residual, the JVP and the VJP stream -- a warp owns a
+// strip of cell columns and marches down the rows, holding the neighbouring
+// rows in registers and the neighbouring columns in its lanes (warp
+// shuffles), so each input is read once per launch and no shared memory or
+// barrier is needed.  Every output has exactly one writer, so results are
+// deterministic (the reference scatters its VJP with float atomics,
 // glide/cuda/residuals.cu:617-1021).
 #include "glide_common.cuh"
 
 namespace glide {
-
-constexpr int TX = 32;               // tile columns (one warp across)
-constexpr int NTHR = 256;            // threads per CTA (32 x 8)
-constexpr int WC = TX + 2;           // window columns (one-cell ring)
-
-struct TileIdx {
-    int i0, j0, tx, ty, tid;
-};
-template <int TYK> __device__ __forceinline__ TileIdx tile_idx() {
-    TileIdx t;
-    t.tx = threadIdx.x % TX;
-    t.ty = threadIdx.x / TX;
-    t.tid = threadIdx.x;
-    t.i0 = blockIdx.y * TYK;
-    t.j0 = blockIdx.x * TX;
-    return t;
-}
 
 // --------------------------------------------------------------------------
 // residual, streaming form (what launch_residual runs).  A warp owns a strip
@@ -477,206 +457,287 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
     }
 }
 
-constexpr int VTY = 8;                   // VJP tile rows (keeps FP64 shared memory < 48 KB)
-constexpr int VRPT = VTY / (NTHR / TX);  // rows per thread = 1
-constexpr int VWR = VTY + 2;
-
 // --------------------------------------------------------------------------
-// VJP lambda^T J in gather form (glide/cuda/residuals.cu:586-1023)
-//
-// The velocity-velocity block is applied as the forward tangent with lambda
-// as the direction (the viscous block is symmetric, residuals.cu:709); the
-// H-row and velocity->H blocks are explicit transposes gathered per output.
-// exact_boundary=0 drops the contributions the reference drops at clamped
-// boundary reads (only non-zero with gl_derivatives), 1 keeps them.
+// VJP lambda^T J, streaming form (what launch_vjp runs): the warp-strip march
+// of jvp_stream_kernel with lambda as the direction.  The velocity-velocity
+// block is applied as the forward tangent (the viscous block is symmetric,
+// glide/cuda/residuals.cu:709); the H rows gather, per cell, the transposed
+// flux, drag and driving partials of its four faces, the eta*H partials of
+// its normal stresses and the vertex weights of its four corner shear
+// stresses.  At iteration i the kernel forms the cell row i+1, the stress
+// tangents of row i and of vertex row i+1, the vertex weights of row i+1 and
+// the H-row contributions of v-face row i+1; the rows above come from the
+// previous iterations (glide/cuda/residuals.cu:586-1023).  exact_boundary = 0
+// drops the contributions the reference drops at clamped boundary reads (only
+// non-zero with gl_derivatives), 1 keeps them.  With RF the output is
+// f - lambda^T J.
 // --------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(NTHR) vjp_kernel(
+#ifndef GLIDE_VS_MINB32
+#define GLIDE_VS_MINB32 1
+#endif
+#ifndef GLIDE_VS_MINB64
+#define GLIDE_VS_MINB64 1
+#endif
+template <typename T, bool RF, typename Ix>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_VS_MINB32 : GLIDE_VS_MINB64) vjp_stream_kernel(
     T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ lu, const T* __restrict__ lv, const T* __restrict__ lH,
-    const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
-    const T* __restrict__ mask, const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H,
-    int residual_form, int exact_boundary, Geo g, Phys<T> p) {
-    __shared__ T s_eta[VWR][WC];
-    __shared__ T s_etaH[VWR][WC];
-    __shared__ T s_detaH[VWR][WC];      // d(eta)(lambda) * H
-    __shared__ T s_dsxx[VTY][WC];
-    __shared__ T s_dsyy[VWR][TX];
-    __shared__ T s_dsxy[VTY + 1][TX + 1];
-    __shared__ T s_W[VTY + 1][TX + 1];  // vertex weight for the H rows of the shear terms
-    __shared__ T s_CuL[VTY][TX + 1], s_CuR[VTY][TX + 1];
-    __shared__ T s_CvT[VTY + 1][TX], s_CvB[VTY + 1][TX];
-
+    const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta, const T* __restrict__ mask,
+    const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, int exact_boundary, Geo g,
+    Phys<T> p, int n_strips, int rows, int n_warps) {
     const int ny = g.ny, nx = g.nx;
-    const int b = blockIdx.z;
+    const int wid = blockIdx.x * (256 / 32) + threadIdx.x / 32;
+    if (wid >= n_warps) return;  // whole warp
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.y;
     u += b * g.nu(); v += b * g.nv(); H += b * g.nc();
     lu += b * g.nu(); lv += b * g.nv(); lH += b * g.nc();
+    if constexpr (RF) { f_u += b * g.nu(); f_v += b * g.nv(); f_H += b * g.nc(); }
     bed += b * g.nc(); B += b * g.nc(); beta += b * g.nc(); mask += b * g.nc();
     o_u += b * g.nu(); o_v += b * g.nv(); o_H += b * g.nc();
-    if (residual_form) { f_u += b * g.nu(); f_v += b * g.nv(); f_H += b * g.nc(); }
-    const TileIdx t = tile_idx<VTY>();
+
+    const int strip = wid % n_strips, chunk = wid / n_strips;
+    const int i0 = chunk * rows;
+    const int i1 = min(i0 + rows, ny);
+    const int jc = strip * SW - 1 + lane;
+    const int jcc = clampi(jc, 0, nx - 1);
+    const int juL = clampi(jc, 0, nx);
+    const int juR = clampi(jc + 1, 0, nx);
+    const int jvL = clampi(jc - 1, 0, nx - 1), jvR = clampi(jc + 1, 0, nx - 1);
+    const bool first = lane == 0, last = lane == 31;
+    const bool own = lane >= 1 && lane <= SW && jc < nx;
+    const unsigned FULL = 0xffffffffu;
     const T dxi = p.dxi;
-    auto lam_t = [&](int i, int j) -> T {  // masked lambda_H (residuals.cu:646)
-        return ldc(lH, i, j, ny, nx) * (T(1) - ldc(mask, i, j, ny, nx));
+    const T rr = rho_ratio<T>();
+    auto Uf = [&](const T* a, int r, int col) -> T {
+        return __ldg(a + Ix(clampi(r, 0, ny - 1)) * (nx + 1) + col);
     };
+    auto Vf = [&](const T* a, int r, int col) -> T { return __ldg(a + Ix(clampi(r, 0, ny)) * nx + col); };
+    auto Cell = [&](const T* a, int r) -> T { return __ldg(a + Ix(clampi(r, 0, ny - 1)) * nx + jcc); };
+    auto slope = [&](T Hx, T bx) -> T { return T(1) + (bx > -rr * Hx ? T(0) : -rr); };
 
-    for (int k = t.tid; k < VWR * WC; k += NTHR) {
-        int r = k / WC, c = k - r * WC;
-        int ic = clampi(t.i0 - 1 + r, 0, ny - 1), jc = clampi(t.j0 - 1 + c, 0, nx - 1);
-        EtaIn<T> ein = eta_inputs(u, v, ic, jc, ny, nx);
-        T Bc = ldc(B, ic, jc, ny, nx);
-        EtaOut<T> e = cell_eta(ein, Bc, ic, jc, ny, nx, p);
-        EtaIn<T> din = eta_inputs(lu, lv, ic, jc, ny, nx);
-        T deta = cell_eta_tangent(e, din, Bc, ic, jc, ny, nx, p);
-        T Hc = ldc(H, ic, jc, ny, nx);
-        s_eta[r][c] = e.eta;
-        s_etaH[r][c] = e.eta * Hc;
-        s_detaH[r][c] = deta * Hc;
-    }
-    __syncthreads();
-
-    for (int k = t.tid; k < VTY * WC; k += NTHR) {
-        int r = k / WC, c = k - r * WC;
-        int i = t.i0 + r, j = t.j0 - 1 + c;
-        NormalStress<T> s = normal_stress<T, true>(ldu(u, i, j, ny, nx), ldu(u, i, j + 1, ny, nx),
-                                                   ldv(v, i, j, ny, nx), ldv(v, i + 1, j, ny, nx),
-                                                   s_etaH[r + 1][c], dxi, j >= 0 && j < nx);
-        s_dsxx[r][c] = s.d_ul * ldu(lu, i, j, ny, nx) + s.d_ur * ldu(lu, i, j + 1, ny, nx) +
-                       s.d_vt * ldv(lv, i, j, ny, nx) + s.d_vb * ldv(lv, i + 1, j, ny, nx) +
-                       s.d_etaH * s_detaH[r + 1][c];
-    }
-    for (int k = t.tid; k < VWR * TX; k += NTHR) {
-        int r = k / TX, c = k - r * TX;
-        int i = t.i0 - 1 + r, j = t.j0 + c;
-        NormalStress<T> s = normal_stress<T, false>(ldu(u, i, j, ny, nx), ldu(u, i, j + 1, ny, nx),
-                                                    ldv(v, i, j, ny, nx), ldv(v, i + 1, j, ny, nx),
-                                                    s_etaH[r][c + 1], dxi, i >= 0 && i < ny);
-        s_dsyy[r][c] = s.d_ul * ldu(lu, i, j, ny, nx) + s.d_ur * ldu(lu, i, j + 1, ny, nx) +
-                       s.d_vt * ldv(lv, i, j, ny, nx) + s.d_vb * ldv(lv, i + 1, j, ny, nx) +
-                       s.d_etaH * s_detaH[r][c + 1];
-    }
-    for (int k = t.tid; k < (VTY + 1) * (TX + 1); k += NTHR) {
-        int r = k / (TX + 1), c = k - r * (TX + 1);
-        int i = t.i0 + r, j = t.j0 + c;
-        T etaH = T(0.25) * (s_etaH[r][c] + s_etaH[r][c + 1] + s_etaH[r + 1][c] + s_etaH[r + 1][c + 1]);
-        T detaH = T(0.25) * (s_detaH[r][c] + s_detaH[r][c + 1] + s_detaH[r + 1][c] + s_detaH[r + 1][c + 1]);
-        bool valid = i > 0 && i < ny && j > 0 && j < nx;
-        ShearStress<T> s = shear_stress(ldu(u, i - 1, j, ny, nx), ldu(u, i, j, ny, nx), ldv(v, i, j - 1, ny, nx),
-                                        ldv(v, i, j, ny, nx), etaH, dxi, valid);
-        s_dsxy[r][c] = s.d_ut * ldu(lu, i - 1, j, ny, nx) + s.d_ub * ldu(lu, i, j, ny, nx) +
-                       s.d_vl * ldv(lv, i, j - 1, ny, nx) + s.d_vr * ldv(lv, i, j, ny, nx) + s.d_etaH * detaH;
-        // the vertex stress enters u(i,j) [+], u(i-1,j) [-], v(i,j) [-], v(i,j-1) [+]
-        T w = valid ? (ldu(lu, i, j, ny, nx) - ldu(lu, i - 1, j, ny, nx) - ldv(lv, i, j, ny, nx) +
-                       ldv(lv, i, j - 1, ny, nx)) * dxi
-                    : T(0);
-        s_W[r][c] = w * s.d_etaH * T(0.25);
-    }
-    // face contributions to the H rows of their two cells
-    for (int k = t.tid; k < VTY * (TX + 1); k += NTHR) {  // u-faces (i,j), j in [j0, j0+TX]
-        int r = k / (TX + 1), c = k - r * (TX + 1);
-        int i = t.i0 + r, j = t.j0 + c;
-        T CL = 0, CR = 0;
-        if (i < ny && j <= nx) {
-            T uf = ldu(u, i, j, ny, nx), lam = ldu(lu, i, j, ny, nx);
-            T H1 = ldc(H, i, j - 1, ny, nx), H2 = ldc(H, i, j, ny, nx);
-            T b1 = ldc(bed, i, j - 1, ny, nx), b2 = ldc(bed, i, j, ny, nx);
-            Flux<T> q = upwind_flux(uf, H1, H2, j > 0 && j < nx);
-            T a = (lam_t(i, j - 1) - lam_t(i, j)) * dxi;
-            BasalDrag<T> tb = basal_drag(uf, H1, H2, b1, b2, ldc(beta, i, j - 1, ny, nx), ldc(beta, i, j, ny, nx), p);
-            Driving<T> td = driving(H1, H2, b1, b2, dxi, j > 0 && j < nx);
-            CL = a * q.d_Ha + lam * (tb.d_H1 - td.d_Hm);
-            CR = a * q.d_Hb + lam * (tb.d_H2 - td.d_Hp);
+    int i = i0 - 2;
+    T uL0 = Uf(u, i, juL), uL1 = Uf(u, i + 1, juL);
+    T uR0 = last ? Uf(u, i, juR) : T(0), uR1 = last ? Uf(u, i + 1, juR) : T(0);
+    T v0 = Vf(v, i, jcc), v1 = Vf(v, i + 1, jcc);
+    T vL1 = first ? Vf(v, i + 1, jvL) : T(0), vR1 = last ? Vf(v, i + 1, jvR) : T(0);
+    T luL0 = Uf(lu, i, juL), luL1 = Uf(lu, i + 1, juL);
+    T luR0 = last ? Uf(lu, i, juR) : T(0), luR1 = last ? Uf(lu, i + 1, juR) : T(0);
+    T lv0 = Vf(lv, i, jcc), lv1 = Vf(lv, i + 1, jcc);
+    T lvL1 = first ? Vf(lv, i + 1, jvL) : T(0), lvR1 = last ? Vf(lv, i + 1, jvR) : T(0);
+    // cell rows m = i-1 and c = i: thickness, grounded fraction, surface, beta,
+    // slope factor, masked lambda_H; row c also its mask and lambda_H
+    T Hm = T(0), gm = T(0), Sm = T(0), bem = T(0), kHm = T(0), ltm = T(0);
+    T Hc = T(0), gcc = T(0), Sc = T(0), bec = T(0), kHc = T(0), ltc = T(0), mc = T(0), lHc = T(0);
+    // eta, eta*H and the tangent of eta*H of row i; stress tangents of row i-1
+    // (syy) and vertex row i (sxy); vertex weights of row i; H-row terms of
+    // v-face row i
+    T eta0 = T(0), etaH0 = T(0), detaH0 = T(0), dsxy0 = T(0), dsyym = T(0), W0 = T(0), CvT0 = T(0), CvB0 = T(0);
+    constexpr bool PREFETCH = sizeof(T) == 4;
+    const int jo = jc < nx ? (jc < 0 ? 0 : jc) : nx - 1;
+    struct RowIn {
+        T uL2, uR2, v2, vL2, vR2, luL2, luR2, lv2, lvL2, lvR2, H, bed, beta, B, lH, m, fu, fv, fH;
+    };
+    auto load_row = [&](int k) {
+        RowIn r;
+        r.uL2 = Uf(u, k + 2, juL);
+        r.uR2 = last ? Uf(u, k + 2, juR) : T(0);
+        r.v2 = Vf(v, k + 2, jcc);
+        r.vL2 = first ? Vf(v, k + 2, jvL) : T(0);
+        r.vR2 = last ? Vf(v, k + 2, jvR) : T(0);
+        r.luL2 = Uf(lu, k + 2, juL);
+        r.luR2 = last ? Uf(lu, k + 2, juR) : T(0);
+        r.lv2 = Vf(lv, k + 2, jcc);
+        r.lvL2 = first ? Vf(lv, k + 2, jvL) : T(0);
+        r.lvR2 = last ? Vf(lv, k + 2, jvR) : T(0);
+        r.H = Cell(H, k + 1); r.bed = Cell(bed, k + 1); r.beta = Cell(beta, k + 1); r.B = Cell(B, k + 1);
+        r.lH = Cell(lH, k + 1); r.m = Cell(mask, k + 1);
+        if constexpr (RF) {
+            const Ix ro = clampi(k, 0, ny - 1);
+            r.fu = __ldg(f_u + ro * (nx + 1) + jo);
+            r.fv = __ldg(f_v + ro * nx + jo);
+            r.fH = __ldg(f_H + ro * nx + jo);
+        } else {
+            r.fu = r.fv = r.fH = T(0);
         }
-        s_CuL[r][c] = CL;
-        s_CuR[r][c] = CR;
-    }
-    for (int k = t.tid; k < (VTY + 1) * TX; k += NTHR) {  // v-faces (i,j), i in [i0, i0+VTY]
-        int r = k / TX, c = k - r * TX;
-        int i = t.i0 + r, j = t.j0 + c;
-        T CT = 0, CB = 0;
-        if (i <= ny && j < nx) {
-            T vf = ldv(v, i, j, ny, nx), lam = ldv(lv, i, j, ny, nx);
-            T Htop = ldc(H, i - 1, j, ny, nx), Hbot = ldc(H, i, j, ny, nx);
-            T btop = ldc(bed, i - 1, j, ny, nx), bbot = ldc(bed, i, j, ny, nx);
-            Flux<T> q = upwind_flux(vf, Hbot, Htop, i > 0 && i < ny);
-            T a = (lam_t(i, j) - lam_t(i - 1, j)) * dxi;
-            BasalDrag<T> tb = basal_drag(vf, Htop, Hbot, btop, bbot, ldc(beta, i - 1, j, ny, nx),
-                                         ldc(beta, i, j, ny, nx), p);
-            Driving<T> td = driving(Hbot, Htop, bbot, btop, dxi, i > 0 && i < ny);
-            CT = a * q.d_Hb + lam * (tb.d_H1 - td.d_Hp);
-            CB = a * q.d_Ha + lam * (tb.d_H2 - td.d_Hm);
+        return r;
+    };
+    RowIn nxt;
+    if constexpr (PREFETCH) nxt = load_row(i);
+    for (; i < i1; ++i) {
+        RowIn cur;
+        if constexpr (PREFETCH) {
+            cur = nxt;
+            nxt = load_row(i + 1);
+        } else {
+            cur = load_row(i);
         }
-        s_CvT[r][c] = CT;
-        s_CvB[r][c] = CB;
-    }
-    __syncthreads();
+        const T Hp = cur.H, bedp = cur.bed, betap = cur.beta, Bp = cur.B;
+        const T mp = cur.m, lHp = cur.lH;
 
-#pragma unroll
-    for (int k = 0; k < VRPT; k++) {
-        const int r = t.ty + k * (NTHR / TX);
-        const int c = t.tx;
-        const int i = t.i0 + r, j = t.j0 + c;
-        if (i >= ny || j >= nx) continue;
-        const int64_t ic = int64_t(i) * nx + j;
-        // ---- H row
+        T uR0s = __shfl_down_sync(FULL, uL0, 1), uR1s = __shfl_down_sync(FULL, uL1, 1);
+        T uR2s = __shfl_down_sync(FULL, cur.uL2, 1);
+        T vL1s = __shfl_up_sync(FULL, v1, 1), vL2s = __shfl_up_sync(FULL, cur.v2, 1);
+        T vR1s = __shfl_down_sync(FULL, v1, 1), vR2s = __shfl_down_sync(FULL, cur.v2, 1);
+        T luR0s = __shfl_down_sync(FULL, luL0, 1), luR1s = __shfl_down_sync(FULL, luL1, 1);
+        T luR2s = __shfl_down_sync(FULL, cur.luL2, 1);
+        T lvL1s = __shfl_up_sync(FULL, lv1, 1), lvL2s = __shfl_up_sync(FULL, cur.lv2, 1);
+        T lvR1s = __shfl_down_sync(FULL, lv1, 1), lvR2s = __shfl_down_sync(FULL, cur.lv2, 1);
+        if (last) {
+            uR0s = uR0; uR1s = uR1; uR2s = cur.uR2; vR1s = vR1; vR2s = cur.vR2;
+            luR0s = luR0; luR1s = luR1; luR2s = cur.luR2; lvR1s = lvR1; lvR2s = cur.lvR2;
+        }
+        if (first) { vL1s = vL1; vL2s = cur.vL2; lvL1s = lvL1; lvL2s = cur.lvL2; }
+
+        // cell row i+1
+        const T gp = sigmoid(bedp + rr * Hp, p.sig_c);
+        const T Sp = M<T>::max(bedp, -rr * Hp) + Hp;
+        const T kHp = slope(Hp, bedp);
+        const T ltp = lHp * (T(1) - mp);
+        T etaP, etaHp, detaHp;
         {
-            const T m = mask[ic];
-            const T lam = lH[ic];
-            const T lamt = lam * (T(1) - m);
-            const T Hc = H[ic];
-            Calving<T> cv = calving(Hc, bed[ic], p);
-            T acc = lamt / p.dt - lamt * cv.d_H;
-            acc += s_CuR[r][c] + s_CuL[r][c + 1] + s_CvB[r][c] + s_CvT[r + 1][c];
-            if (exact_boundary) {
-                if (j == 0) acc += s_CuL[r][c];            // face 0 read H(i,-1) -> H(i,0)
-                if (j == nx - 1) acc += s_CuR[r][c + 1];   // face nx read H(i,nx) -> H(i,nx-1)
-                if (i == 0) acc += s_CvT[r][c];
-                if (i == ny - 1) acc += s_CvB[r + 1][c];
+            EtaIn<T> a, da;
+            a.ul = uL1;   a.ur = uR1s;  a.vt = v1;    a.vb = cur.v2;
+            a.u_tl = uL0; a.u_tr = uR0s; a.u_bl = cur.uL2; a.u_br = uR2s;
+            a.v_lt = vL1s; a.v_rt = vR1s; a.v_lb = vL2s; a.v_rb = vR2s;
+            da.ul = luL1;   da.ur = luR1s;  da.vt = lv1;    da.vb = cur.lv2;
+            da.u_tl = luL0; da.u_tr = luR0s; da.u_bl = cur.luL2; da.u_br = luR2s;
+            da.v_lt = lvL1s; da.v_rt = lvR1s; da.v_lb = lvL2s; da.v_rb = lvR2s;
+            const int ie = clampi(i + 1, 0, ny - 1);
+            const EtaOut<T> e = cell_eta(a, Bp, ie, jcc, ny, nx, p);
+            const T deta = cell_eta_tangent(e, da, Bp, ie, jcc, ny, nx, p);
+            etaP = e.eta;
+            etaHp = e.eta * Hp;
+            detaHp = deta * Hp;
+        }
+
+        // stress tangents of row i, vertex row i+1 (with its H-row weight)
+        T dsxx, dsyy, hx, hy;
+        {
+            const NormalStress<T> s = normal_stress<T, true>(uL0, uR0s, v0, v1, etaH0, dxi, jc >= 0 && jc < nx);
+            dsxx = s.d_ul * luL0 + s.d_ur * luR0s + s.d_vt * lv0 + s.d_vb * lv1 + s.d_etaH * detaH0;
+            hx = s.d_etaH;
+        }
+        {
+            const NormalStress<T> s = normal_stress<T, false>(uL0, uR0s, v0, v1, etaH0, dxi, i >= 0 && i < ny);
+            dsyy = s.d_ul * luL0 + s.d_ur * luR0s + s.d_vt * lv0 + s.d_vb * lv1 + s.d_etaH * detaH0;
+            hy = s.d_etaH;
+        }
+        T dsxy1, W1;
+        {
+            const T etaH0L = __shfl_up_sync(FULL, etaH0, 1), etaHpL = __shfl_up_sync(FULL, etaHp, 1);
+            const T detaH0L = __shfl_up_sync(FULL, detaH0, 1), detaHpL = __shfl_up_sync(FULL, detaHp, 1);
+            const bool valid = i + 1 > 0 && i + 1 < ny && jc > 0 && jc < nx;
+            const ShearStress<T> s = shear_stress(uL0, uL1, vL1s, v1, T(0.25) * (etaH0L + etaH0 + etaHpL + etaHp),
+                                                  dxi, valid);
+            const T detaH = T(0.25) * (detaH0L + detaH0 + detaHpL + detaHp);
+            dsxy1 = s.d_ut * luL0 + s.d_ub * luL1 + s.d_vl * lvL1s + s.d_vr * lv1 + s.d_etaH * detaH;
+            const T w = valid ? (luL1 - luL0 - lv1 + lvL1s) * dxi : T(0);
+            W1 = w * s.d_etaH * T(0.25);
+        }
+        // H-row terms of v-face row i+1 (top cell: row i, bottom cell: row i+1)
+        T CvT1, CvB1;
+        {
+            const bool valid = i + 1 > 0 && i + 1 < ny;
+            const Flux<T> q = upwind_flux(v1, Hp, Hc, valid);
+            const T a = (ltp - ltc) * dxi;
+            const BasalDrag<T> tb = basal_drag_g(v1, gcc, gp, bec, betap, p);
+            const T w = valid ? T(1) : T(0);     // driving: m = bottom (row i+1), p = top (row i)
+            const T dS = Sc - Sp, Havg = T(0.5) * (Hp + Hc);
+            const T d_Hm = (T(0.5) * dS * dxi - Havg * kHp * dxi) * w;
+            const T d_Hp = (T(0.5) * dS * dxi + Havg * kHc * dxi) * w;
+            CvT1 = a * q.d_Hb + lv1 * (tb.d_H1 - d_Hp);
+            CvB1 = a * q.d_Ha + lv1 * (tb.d_H2 - d_Hm);
+        }
+
+        if (i >= i0) {  // warp-uniform
+            const T HcL = __shfl_up_sync(FULL, Hc, 1);
+            const T gcL = __shfl_up_sync(FULL, gcc, 1), gcR = __shfl_down_sync(FULL, gcc, 1);
+            const T ScL = __shfl_up_sync(FULL, Sc, 1), kHcL = __shfl_up_sync(FULL, kHc, 1);
+            const T becL = __shfl_up_sync(FULL, bec, 1), becR = __shfl_down_sync(FULL, bec, 1);
+            const T ltL = __shfl_up_sync(FULL, ltc, 1);
+            // H-row terms of u-face (i, jc) (left cell: jc-1, right cell: jc)
+            T CuL, CuR;
+            {
+                const bool valid = jc > 0 && jc < nx;
+                const Flux<T> q = upwind_flux(uL0, HcL, Hc, valid);
+                const T a = (ltL - ltc) * dxi;
+                const BasalDrag<T> tb = basal_drag_g(uL0, gcL, gcc, becL, bec, p);
+                const T w = valid ? T(1) : T(0);  // driving: m = left, p = right
+                const T dS = Sc - ScL, Havg = T(0.5) * (HcL + Hc);
+                const T d_Hm = (T(0.5) * dS * dxi - Havg * kHcL * dxi) * w;
+                const T d_Hp = (T(0.5) * dS * dxi + Havg * kHc * dxi) * w;
+                CuL = a * q.d_Ha + luL0 * (tb.d_H1 - d_Hm);
+                CuR = a * q.d_Hb + luL0 * (tb.d_H2 - d_Hp);
             }
-            const T eta = s_eta[r + 1][c + 1], etaH = s_etaH[r + 1][c + 1];
-            const T ul = u[int64_t(i) * (nx + 1) + j], ur = u[int64_t(i) * (nx + 1) + j + 1];
-            const T vt = v[ic], vb = v[int64_t(i + 1) * nx + j];
-            NormalStress<T> sx = normal_stress<T, true>(ul, ur, vt, vb, etaH, dxi, true);
-            NormalStress<T> sy = normal_stress<T, false>(ul, ur, vt, vb, etaH, dxi, true);
-            const T lul = lu[int64_t(i) * (nx + 1) + j], lur = lu[int64_t(i) * (nx + 1) + j + 1];
-            const T lvt = lv[ic], lvb = lv[int64_t(i + 1) * nx + j];
-            acc += (lul - lur) * sx.d_etaH * eta * dxi;
-            acc += (lvb - lvt) * sy.d_etaH * eta * dxi;
-            acc += eta * (s_W[r][c] + s_W[r][c + 1] + s_W[r + 1][c] + s_W[r + 1][c + 1]);
-            acc += lam * m;
-            o_H[ic] = residual_form ? f_H[ic] - acc : acc;
+            const T CuLR = __shfl_down_sync(FULL, CuL, 1), CuRR = __shfl_down_sync(FULL, CuR, 1);
+            const T dsxxL = __shfl_up_sync(FULL, dsxx, 1), dsxxR = __shfl_down_sync(FULL, dsxx, 1);
+            const T dsxy0R = __shfl_down_sync(FULL, dsxy0, 1), dsxy1R = __shfl_down_sync(FULL, dsxy1, 1);
+            const T W0R = __shfl_down_sync(FULL, W0, 1), W1R = __shfl_down_sync(FULL, W1, 1);
+            const T ltR = __shfl_down_sync(FULL, ltc, 1);
+            if (own) {
+                const Ix ic = Ix(i) * nx + jc;
+                // ---- H row
+                {
+                    const Calving<T> cv = calving_g(Hc, gcc, p);
+                    T acc = ltc / p.dt - ltc * cv.d_H;
+                    acc += CuR + CuLR + CvB0 + CvT1;
+                    if (exact_boundary) {
+                        if (jc == 0) acc += CuL;
+                        if (jc == nx - 1) acc += CuRR;
+                        if (i == 0) acc += CvT0;
+                        if (i == ny - 1) acc += CvB1;
+                    }
+                    acc += (luL0 - luR0s) * hx * eta0 * dxi;
+                    acc += (lv1 - lv0) * hy * eta0 * dxi;
+                    acc += eta0 * (W0 + W0R + W1 + W1R);
+                    acc += lHc * mc;
+                    o_H[ic] = RF ? cur.fH - acc : acc;
+                }
+                // ---- u-face (i, jc) and, at the right edge, (i, nx)
+                {
+                    T val = (dsxx - dsxxL) * dxi + (dsxy0 - dsxy1) * dxi;
+                    const BasalDrag<T> tb = basal_drag_g(uL0, gcL, gcc, becL, bec, p);
+                    const Flux<T> q = upwind_flux(uL0, HcL, Hc, jc > 0 && jc < nx);
+                    val += luL0 * tb.d_vel + (ltL - ltc) * dxi * q.d_vel;
+                    o_u[Ix(i) * (nx + 1) + jc] = RF ? cur.fu - val : val;
+                    if (jc == nx - 1) {
+                        T ve = (dsxxR - dsxx) * dxi + (dsxy0R - dsxy1R) * dxi;
+                        const BasalDrag<T> te = basal_drag_g(uR0s, gcc, gcR, bec, becR, p);
+                        const Flux<T> qe = upwind_flux(uR0s, Hc, Hc, false);  // H(i, nx) clamps to H(i, nx-1)
+                        ve += luR0s * te.d_vel + (ltc - ltR) * dxi * qe.d_vel;
+                        const Ix oe = Ix(i) * (nx + 1) + nx;
+                        o_u[oe] = RF ? __ldg(f_u + oe) - ve : ve;
+                    }
+                }
+                // ---- v-face (i, jc) and, at the bottom edge, (ny, jc)
+                {
+                    T val = (dsyym - dsyy) * dxi + (dsxy0R - dsxy0) * dxi;
+                    const BasalDrag<T> tb = basal_drag_g(v0, gm, gcc, bem, bec, p);
+                    const Flux<T> q = upwind_flux(v0, Hc, Hm, i > 0 && i < ny);
+                    val += lv0 * tb.d_vel + (ltc - ltm) * dxi * q.d_vel;
+                    o_v[ic] = RF ? cur.fv - val : val;
+                    if (i == ny - 1) {
+                        T ve = (dsyy - T(0)) * dxi + (dsxy1R - dsxy1) * dxi;
+                        const BasalDrag<T> te = basal_drag_g(v1, gcc, gp, bec, betap, p);
+                        const Flux<T> qe = upwind_flux(v1, Hp, Hc, false);
+                        ve += lv1 * te.d_vel + (ltp - ltc) * dxi * qe.d_vel;
+                        const Ix oe = Ix(ny) * nx + jc;
+                        o_v[oe] = RF ? __ldg(f_v + oe) - ve : ve;
+                    }
+                }
+            }
         }
-        // ---- u-faces
-        for (int e = 0; e < 2; e++) {
-            const int jj = j + e;
-            if (e == 1 && jj != nx) break;
-            const int cc = c + e;
-            T val = (s_dsxx[r][cc + 1] - s_dsxx[r][cc]) * dxi + (s_dsxy[r][cc] - s_dsxy[r + 1][cc]) * dxi;
-            const T uf = ldu(u, i, jj, ny, nx), lam = ldu(lu, i, jj, ny, nx);
-            const T H1 = ldc(H, i, jj - 1, ny, nx), H2 = ldc(H, i, jj, ny, nx);
-            BasalDrag<T> tb = basal_drag(uf, H1, H2, ldc(bed, i, jj - 1, ny, nx), ldc(bed, i, jj, ny, nx),
-                                         ldc(beta, i, jj - 1, ny, nx), ldc(beta, i, jj, ny, nx), p);
-            Flux<T> q = upwind_flux(uf, H1, H2, jj > 0 && jj < nx);
-            val += lam * tb.d_vel + (lam_t(i, jj - 1) - lam_t(i, jj)) * dxi * q.d_vel;
-            const int64_t iu = int64_t(i) * (nx + 1) + jj;
-            o_u[iu] = residual_form ? f_u[iu] - val : val;
-        }
-        // ---- v-faces
-        for (int e = 0; e < 2; e++) {
-            const int ii = i + e;
-            if (e == 1 && ii != ny) break;
-            const int rr = r + e;
-            T val = (s_dsyy[rr][c] - s_dsyy[rr + 1][c]) * dxi + (s_dsxy[rr][c + 1] - s_dsxy[rr][c]) * dxi;
-            const T vf = ldv(v, ii, j, ny, nx), lam = ldv(lv, ii, j, ny, nx);
-            const T Htop = ldc(H, ii - 1, j, ny, nx), Hbot = ldc(H, ii, j, ny, nx);
-            BasalDrag<T> tb = basal_drag(vf, Htop, Hbot, ldc(bed, ii - 1, j, ny, nx), ldc(bed, ii, j, ny, nx),
-                                         ldc(beta, ii - 1, j, ny, nx), ldc(beta, ii, j, ny, nx), p);
-            Flux<T> q = upwind_flux(vf, Hbot, Htop, ii > 0 && ii < ny);
-            val += lam * tb.d_vel + (lam_t(ii, j) - lam_t(ii - 1, j)) * dxi * q.d_vel;
-            const int64_t iv = int64_t(ii) * nx + j;
-            o_v[iv] = residual_form ? f_v[iv] - val : val;
-        }
+        // roll the window one row down
+        dsyym = dsyy; dsxy0 = dsxy1; W0 = W1; CvT0 = CvT1; CvB0 = CvB1;
+        eta0 = etaP; etaH0 = etaHp; detaH0 = detaHp;
+        Hm = Hc; gm = gcc; Sm = Sc; bem = bec; kHm = kHc; ltm = ltc;
+        Hc = Hp; gcc = gp; Sc = Sp; bec = betap; kHc = kHp; ltc = ltp; mc = mp; lHc = lHp;
+        uL0 = uL1; uL1 = cur.uL2; uR0 = uR1; uR1 = cur.uR2;
+        v0 = v1; v1 = cur.v2; vL1 = cur.vL2; vR1 = cur.vR2;
+        luL0 = luL1; luL1 = cur.luL2; luR0 = luR1; luR1 = cur.luR2;
+        lv0 = lv1; lv1 = cur.lv2; lvL1 = cur.lvL2; lvR1 = cur.lvR2;
     }
 }
 
@@ -724,7 +785,6 @@ __global__ void grad_beta_kernel(T* __restrict__ grad, const T* __restrict__ u, 
 // --------------------------------------------------------------------------
 // launchers
 // --------------------------------------------------------------------------
-static inline dim3 tile_grid(const Geo& g, int ty) { return dim3((g.nx + TX - 1) / TX, (g.ny + ty - 1) / ty, g.nb); }
 
 // strips of SW columns, row chunks sized for ~32 warps per SM
 struct StreamShape {
@@ -791,11 +851,19 @@ int launch_vjp(const GlideLevelArgs* a, const void* l_u, const void* l_v, const 
                cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
-    int rf = f_u != nullptr;
-    glide::count_launch(), vjp_kernel<T><<<tile_grid(g, VTY), NTHR, 0, s>>>(
-        (T*)o_u, (T*)o_v, (T*)o_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)l_u, (const T*)l_v,
-        (const T*)l_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask, (const T*)f_u,
-        (const T*)f_v, (const T*)f_H, rf, exact_boundary, g, p);
+    const StreamShape sh = stream_shape(g);
+    const dim3 grid((sh.n_warps + 7) / 8, g.nb);
+    auto go = [&](auto kernel) {
+        glide::count_launch(), kernel<<<grid, 256, 0, s>>>(
+            (T*)o_u, (T*)o_v, (T*)o_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)l_u,
+            (const T*)l_v, (const T*)l_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
+            (const T*)f_u, (const T*)f_v, (const T*)f_H, exact_boundary, g, p, sh.n_strips, sh.rows, sh.n_warps);
+    };
+    const bool i32 = index32(g);
+    if (f_u != nullptr)
+        i32 ? go(vjp_stream_kernel<T, true, int>) : go(vjp_stream_kernel<T, true, int64_t>);
+    else
+        i32 ? go(vjp_stream_kernel<T, false, int>) : go(vjp_stream_kernel<T, false, int64_t>);
     return (int)cudaGetLastError();
 }
 

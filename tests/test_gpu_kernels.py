@@ -134,10 +134,11 @@ def test_jvp_batch_matches_single():
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("gl,exact", [(False, False), (True, False), (True, True)])
-def test_vjp(precision, gl, exact):
+@pytest.mark.parametrize("shape", [(32, 32), (24, 40), (33, 47), (70, 100), (5, 3), (130, 61)])
+def test_vjp(precision, gl, exact, shape):
     import torch
     from oracle import ssa
-    st = _state((32, 32), seed=2)
+    st = _state(shape, seed=2)
     g = _grid(st, precision, gl_derivatives=gl)
     g.lambda_u.copy_(torch.as_tensor(st["d_u"]))
     g.lambda_v.copy_(torch.as_tensor(st["d_v"]))
@@ -147,6 +148,47 @@ def test_vjp(precision, gl, exact):
                   st["mask"], st["gamma"], _params(gl), st["dx"], st["dt"], exact_boundary=exact)
     for a, b in zip((g.l_u, g.l_v, g.l_H), ref):
         assert _rel(_np(a), b) <= TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vjp_residual_form(precision):
+    """glide_vjp with f writes f - lambda^T J (the adjoint residual)."""
+    import ctypes as C
+    from glide_b200 import _native as N
+    st = _state((70, 100), seed=6)
+    g = _grid(st, precision, gl_derivatives=True)
+    g.lambda_u.copy_(torch.as_tensor(st["d_u"]))
+    g.lambda_v.copy_(torch.as_tensor(st["d_v"]))
+    g.lambda_H.copy_(torch.as_tensor(st["d_H"]))
+    g.compute_vjp(exact_boundary=True)
+    a = g.level_args()
+    out = [torch.full_like(t, float("nan")) for t in (g.l_u, g.l_v, g.l_H)]
+    N.check(N.load().glide_vjp(C.byref(a), g.lambda_u.data_ptr(), g.lambda_v.data_ptr(), g.lambda_H.data_ptr(),
+                               g.f_u.data_ptr(), g.f_v.data_ptr(), g.f_H.data_ptr(), out[0].data_ptr(),
+                               out[1].data_ptr(), out[2].data_ptr(), 1, N.stream_handle()), "vjp")
+    eps = torch.finfo(g.dtype).eps
+    for o, f, l in zip(out, (g.f_u, g.f_v, g.f_H), (g.l_u, g.l_v, g.l_H)):
+        assert float((o - (f - l)).abs().max()) <= 8 * eps * float((f.abs() + l.abs()).max())
+
+
+def test_vjp_batch_matches_single():
+    """A batch of 3 problems gives the same VJP as 3 single calls."""
+    from glide_b200.grid import Grid
+    sts = [_state((33, 47), seed=s) for s in (30, 31, 32)]
+    g = Grid(33, 47, sts[0]["dx"], dt=10.0, dtype=torch.float32, nb=3, gl_derivatives=True)
+    for k in ("u", "v", "H", "bed", "B", "beta", "mask", "gamma"):
+        getattr(g, k).copy_(torch.as_tensor(np.stack([s[k] for s in sts])))
+    g.lambda_u.copy_(torch.as_tensor(np.stack([s["d_u"] for s in sts])))
+    g.lambda_v.copy_(torch.as_tensor(np.stack([s["d_v"] for s in sts])))
+    g.lambda_H.copy_(torch.as_tensor(np.stack([s["d_H"] for s in sts])))
+    g.compute_vjp(exact_boundary=True)
+    for b, st in enumerate(sts):
+        g1 = _grid(st, "fp32", gl_derivatives=True)
+        g1.lambda_u.copy_(torch.as_tensor(st["d_u"]))
+        g1.lambda_v.copy_(torch.as_tensor(st["d_v"]))
+        g1.lambda_H.copy_(torch.as_tensor(st["d_H"]))
+        g1.compute_vjp(exact_boundary=True)
+        assert torch.equal(g.l_u[b], g1.l_u) and torch.equal(g.l_v[b], g1.l_v) and torch.equal(g.l_H[b], g1.l_H)
 
 
 def test_vjp_dot_jvp_fp64():
