@@ -472,14 +472,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_JS_MINB32 : GLIDE_
 // non-zero with gl_derivatives), 1 keeps them.  With RF the output is
 // f - lambda^T J.
 // --------------------------------------------------------------------------
+// 128-thread CTAs: with 150-180 registers per thread three fit on an SM in
+// FP32 (12 warps; one 256-thread CTA would give 8), two in FP64
+constexpr int VS_NT = 128;
 #ifndef GLIDE_VS_MINB32
-#define GLIDE_VS_MINB32 1
+#define GLIDE_VS_MINB32 3
 #endif
 #ifndef GLIDE_VS_MINB64
-#define GLIDE_VS_MINB64 1
+#define GLIDE_VS_MINB64 2
 #endif
 template <typename T, bool RF, typename Ix>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_VS_MINB32 : GLIDE_VS_MINB64) vjp_stream_kernel(
+__global__ void __launch_bounds__(VS_NT, sizeof(T) == 4 ? GLIDE_VS_MINB32 : GLIDE_VS_MINB64) vjp_stream_kernel(
     T* __restrict__ o_u, T* __restrict__ o_v, T* __restrict__ o_H,
     const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ lu, const T* __restrict__ lv, const T* __restrict__ lH,
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? GLIDE_VS_MINB32 : GLIDE_
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, int exact_boundary, Geo g,
     Phys<T> p, int n_strips, int rows, int n_warps) {
     const int ny = g.ny, nx = g.nx;
-    const int wid = blockIdx.x * (256 / 32) + threadIdx.x / 32;
+    const int wid = blockIdx.x * (VS_NT / 32) + threadIdx.x / 32;
     if (wid >= n_warps) return;  // whole warp
     const int lane = threadIdx.x & 31;
     const int b = blockIdx.y;
@@ -852,9 +855,9 @@ int launch_vjp(const GlideLevelArgs* a, const void* l_u, const void* l_v, const 
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
     const StreamShape sh = stream_shape(g);
-    const dim3 grid((sh.n_warps + 7) / 8, g.nb);
+    const dim3 grid((sh.n_warps + VS_NT / 32 - 1) / (VS_NT / 32), g.nb);
     auto go = [&](auto kernel) {
-        glide::count_launch(), kernel<<<grid, 256, 0, s>>>(
+        glide::count_launch(), kernel<<<grid, VS_NT, 0, s>>>(
             (T*)o_u, (T*)o_v, (T*)o_H, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)l_u,
             (const T*)l_v, (const T*)l_H, (const T*)a->bed, (const T*)a->B, (const T*)a->beta, (const T*)a->mask,
             (const T*)f_u, (const T*)f_v, (const T*)f_H, exact_boundary, g, p, sh.n_strips, sh.rows, sh.n_warps);
