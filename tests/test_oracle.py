@@ -152,3 +152,21 @@ def test_pivoted_local_solve_matches_dense_solve():
     with np.errstate(divide="ignore", invalid="ignore"):
         xu = np.stack(lu5_solve(A, b)).T
     assert not np.isfinite(xu[:8]).all()
+
+
+def test_oracle_check_relative_residuals():
+    """The checker's |r| / |r0|: 1 for the starting state, the direct
+    evaluation for another state, the same with worker processes."""
+    from glide_b200.synthetic import dome_case
+    from oracle.check import relative_residuals, residual_parts
+    c = dome_case(2, n=32, dx=10000.0)
+    rng = np.random.default_rng(5)
+    state = (rng.standard_normal((32, 33)) * 20, rng.standard_normal((33, 32)) * 20, c.thickness + 3.0)
+    geo = dict(bed=c.bed, B=c.B, beta=c.beta, H_prev=c.thickness, smb=c.smb, dx=c.dx, dt=c.dt, thklim=c.thklim)
+    start = (np.zeros((32, 33)), np.zeros((33, 32)), c.thickness)
+    r0 = np.sqrt(sum(residual_parts(*start, c.bed, c.B, c.beta, c.thickness, c.smb, c.dx, c.dt)))
+    r1 = np.sqrt(sum(residual_parts(*state, c.bed, c.B, c.beta, c.thickness, c.smb, c.dx, c.dt)))
+    serial = relative_residuals([(geo, [start, state])], workers=1)
+    assert serial[0][0] == 1.0 and abs(serial[0][1] - r1 / r0) <= 1e-15 * r1 / r0
+    par = relative_residuals([(geo, [state]), (geo, [start])], workers=2)
+    assert par == [[serial[0][1]], [1.0]]
