@@ -12,9 +12,14 @@
 //  * capacity: NOALLOC_SCRATCH_BYTES = 10 MiB, i.e. 5 deltas per cell for at
 //    most 262,144 cells (nb * ny * nx) in FP64 or 524,288 cells in FP32;
 //    larger problems are rejected with GLIDE_E_TOO_LARGE before any launch;
-//  * the device address of the array is looked up once per device, on the
-//    first call made with that device current (cudaGetSymbolAddress); make
-//    that first call before any stream capture on that device;
+//  * the device address of the array is looked up on the first call made
+//    with a device current (cudaGetSymbolAddress) and cached together with
+//    the unique id of the CUDA context it belongs to; a later call in another
+//    context of that device (after cudaDeviceReset, or once the primary
+//    context was released and created again, when the library's module and
+//    so the array may have moved) looks it up again.  Make the first call on
+//    a device, and the first call after such a reset, before any stream
+//    capture on that device;
 //  * all calls share the one array: calls that overlap on the GPU (other
 //    streams, other host threads) race on it and must be ordered by the
 //    caller; the array keeps the last call's contents, and nothing needs
@@ -40,24 +45,65 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mutex;
-void* g_scratch_ptr[MAX_DEVICES] = {nullptr};
+struct Cached {
+    unsigned long long ctx_id;  // unique id of the context the address belongs to (cuCtxGetId)
+    void* ptr;
+};
+Cached g_cache[MAX_DEVICES] = {};
 
-// Device address of the scratch array on the current device (set-up on the
-// first call per device).  In host code the symbol itself is only a host-side
-// stand-in, so the address must come from cudaGetSymbolAddress.
+// Driver queries reached through the runtime (no link against libcuda):
+// CUresult cuCtxGetCurrent(CUcontext*), CUresult cuCtxGetId(CUcontext, unsigned long long*).
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+std::once_flag g_entry_once;
+
+void load_entry_points() {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_id = reinterpret_cast<CtxGetIdFn>(f);
+}
+
+// Id of the context current on this thread; 0 if there is none (or it
+// cannot be queried, in which case the address is looked up every call).
+unsigned long long current_ctx_id() {
+    std::call_once(g_entry_once, load_entry_points);
+    if (!g_ctx_current || !g_ctx_id) return 0;
+    void* ctx = nullptr;
+    if (g_ctx_current(&ctx) != 0 || ctx == nullptr) return 0;
+    unsigned long long id = 0;
+    if (g_ctx_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch array in the current context.  In host code
+// the symbol itself is only a host-side stand-in, so the address must come
+// from cudaGetSymbolAddress.
 int scratch_address(void** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return int(e);
     if (dev < 0 || dev >= MAX_DEVICES) return GLIDE_E_SHAPE;
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (g_scratch_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return int(e);
-        g_scratch_ptr[dev] = p;
+    Cached& c = g_cache[dev];
+    const unsigned long long id = current_ctx_id();
+    if (c.ptr != nullptr && id != 0 && id == c.ctx_id) {
+        *out = c.ptr;
+        return 0;
     }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);   // also creates the context on a first call
+    if (e != cudaSuccess) return int(e);
+    c.ptr = p;
+    c.ctx_id = id != 0 ? id : current_ctx_id();
+    *out = p;
     return 0;
 }
 
