@@ -26,6 +26,8 @@ SYMBOLS = [
     "glide_graph_destroy", "glide_launch_count", "glide_version", "glide_vanka_sweeps_noalloc",
     "glide_noalloc_scratch_bytes", "glide_vanka_sweeps_ex", "glide_vanka_lu", "glide_vanka_linear",
     "glide_misfit", "glide_tikhonov", "glide_loss_parts", "glide_jvp_add",
+    "glide_linear_setup", "glide_linear_vcycle", "glide_vanka_lu_masked", "glide_newton_rhs", "glide_newton_update",
+    "glide_active_mask", "glide_dots", "glide_dots_parts", "glide_combine",
 ]
 
 
@@ -50,7 +52,9 @@ class Level(C.Structure):
                 ("lam", C.c_void_p), ("f_adj", C.c_void_p), ("r_adj", C.c_void_p),
                 ("H_prev", C.c_void_p), ("smb", C.c_void_p),
                 ("scratch", C.c_void_p), ("flags", C.c_void_p), ("any_active", C.c_void_p),
-                ("ls_tmp", C.c_void_p), ("ls_norms", C.c_void_p), ("norm_parts", C.c_void_p)]
+                ("ls_tmp", C.c_void_p), ("ls_norms", C.c_void_p), ("norm_parts", C.c_void_p),
+                ("lu", C.c_void_p), ("lin_rhs", C.c_void_p), ("lin_rho", C.c_void_p), ("lin_d", C.c_void_p),
+                ("r_raw", C.c_void_p)]
 
 LS_CANDIDATES = 4  # GLIDE_LS_CANDIDATES
 
@@ -60,7 +64,9 @@ class SolverConfig(C.Structure):
                 ("n_local", C.c_int), ("n_newton", C.c_int), ("omega", C.c_double), ("shift", C.c_double),
                 ("err_threshold", C.c_double), ("adj_coarse", C.c_int), ("adj_smooth", C.c_int),
                 ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int),
-                ("newton_step", C.c_double), ("pivoted_lu", C.c_int), ("coarse_line_search", C.c_int)]
+                ("newton_step", C.c_double), ("pivoted_lu", C.c_int), ("coarse_line_search", C.c_int),
+                ("lin_pre", C.c_int), ("lin_post", C.c_int), ("lin_coarse", C.c_int), ("lin_omega", C.c_double),
+                ("lin_shift", C.c_double)]
 
 
 class NativeError(RuntimeError):
@@ -116,6 +122,15 @@ def load():
         "glide_vanka_sweeps_noalloc": [LA, vp, vp, vp, i, i, d, d, vp, vp, vp],
         "glide_noalloc_scratch_bytes": [],
         "glide_version": [],
+        "glide_linear_setup": [C.POINTER(Level), i, C.POINTER(SolverConfig), vp],
+        "glide_linear_vcycle": [C.POINTER(Level), i, C.POINTER(SolverConfig), vp],
+        "glide_vanka_lu_masked": [LA, vp, d, vp],
+        "glide_newton_rhs": [LA, vp, vp, vp, vp, vp],
+        "glide_newton_update": [LA, vp, vp, vp, d, vp],
+        "glide_active_mask": [LA, vp, vp, vp],
+        "glide_dots": [i, i64, i, vp, i64, vp, vp, vp, vp],
+        "glide_dots_parts": [i64],
+        "glide_combine": [i, i64, i, vp, i64, vp, d, vp, d, vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

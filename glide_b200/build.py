@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libglide_b200.so"
 SOURCES = ["ssa_stencil.cu", "vanka.cu", "transfer.cu", "driver.cu", "tc_gemm.cu", "unet_ops.cu",
-           "vanka_noalloc.cu", "losses.cu"]
+           "vanka_noalloc.cu", "losses.cu", "krylov.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -155,6 +155,14 @@ int glide_vanka_lu(const GlideLevelArgs* a, const void* f_H, void* lu, double sh
                      launch_vanka_lu<double>(a, f_H, lu, shift, S(stream)));
 }
 
+int glide_vanka_lu_masked(const GlideLevelArgs* a, void* lu, double shift, void* stream) {
+    int e = check_level(a);
+    if (e) return e;
+    if (!lu) return GLIDE_E_NULL;
+    return TDISPATCH(a->dtype, launch_vanka_lu<float>(a, nullptr, lu, shift, S(stream)),
+                     launch_vanka_lu<double>(a, nullptr, lu, shift, S(stream)));
+}
+
 int glide_vanka_linear(const GlideLevelArgs* a, const void* rho_u, const void* rho_v, const void* rho_H,
                        const void* lu, void* d_u, void* d_v, void* d_H, double omega, void* scratch, void* stream) {
     int e = check_level(a);
@@ -478,6 +486,64 @@ int adjoint(GlideLevel* lv, int n, int k, const GlideSolverConfig* c, void* s) {
     return mask_off(L, s);
 }
 
+// --- linear multigrid of the Newton-Krylov finishing solver -------------------
+int lin_ready(GlideLevel* lv, int n) {
+    for (int k = 0; k < n; k++)
+        if (!lv[k].lu || !lv[k].lin_rhs || !lv[k].lin_rho || !lv[k].lin_d || !lv[k].r_raw || !lv[k].scratch)
+            return GLIDE_E_NULL;
+    return 0;
+}
+
+int linear_setup(GlideLevel* lv, int n, const GlideSolverConfig* c, void* s) {
+    TRY(fill_gamma(&lv[0], c->thklim, s));
+    for (int k = 1; k < n; k++) {
+        GlideLevel *F = &lv[k - 1], *L = &lv[k];
+        LevelView w = view(L);
+        TRY(restrict3(F, L, F->U, L->U, s));
+        TRY(restrict3(F, L, F->r_raw, L->r_raw, s));
+        TRY(fill_gamma(L, c->thklim, s));
+        TRY(glide_active_mask(&L->a, w.H(L->r_raw), (void*)L->a.mask, s));
+    }
+    for (int k = 0; k < n; k++) TRY(glide_vanka_lu_masked(&lv[k].a, lv[k].lu, c->lin_shift, s));
+    return 0;
+}
+
+// rho = rhs + J d on level L
+int lin_residual(GlideLevel* L, void* s) {
+    LevelView w = view(L);
+    return glide_jvp_add(&L->a, w.u(L->lin_d), w.v(L->lin_d), w.H(L->lin_d), w.u(L->lin_rhs), w.v(L->lin_rhs),
+                         w.H(L->lin_rhs), w.u(L->lin_rho), w.v(L->lin_rho), w.H(L->lin_rho), s);
+}
+
+int lin_sweeps(GlideLevel* L, int n_sweeps, bool from_zero, const GlideSolverConfig* c, void* s) {
+    LevelView w = view(L);
+    for (int it = 0; it < n_sweeps; it++) {
+        void* rho = L->lin_rho;
+        if (it == 0 && from_zero) rho = L->lin_rhs;   // d = 0: rho = rhs
+        else TRY(lin_residual(L, s));
+        TRY(glide_vanka_linear(&L->a, w.u(rho), w.v(rho), w.H(rho), L->lu, w.u(L->lin_d), w.v(L->lin_d),
+                               w.H(L->lin_d), c->lin_omega, L->scratch, s));
+    }
+    return 0;
+}
+
+int lin_vcycle(GlideLevel* lv, int n, int k, const GlideSolverConfig* c, void* s) {
+    GlideLevel* L = &lv[k];
+    LevelView w = view(L);
+    TRY(glide_fill(w.dt, L->lin_d, 0.0, w.ntot * w.nb, s));
+    if (k == n - 1) return lin_sweeps(L, c->lin_coarse, true, c, s);
+    TRY(lin_sweeps(L, c->lin_pre, true, c, s));
+    GlideLevel* C = &lv[k + 1];
+    LevelView wc = view(C);
+    TRY(lin_residual(L, s));
+    TRY(restrict3(L, C, L->lin_rho, C->lin_rhs, s));
+    TRY(lin_vcycle(lv, n, k + 1, c, s));
+    TRY(glide_prolong(w.dt, 0, 1, 1, wc.u(C->lin_d), w.u(L->lin_d), C->a.ny, C->a.nx, C->a.nb, s));
+    TRY(glide_prolong(w.dt, 1, 1, 1, wc.v(C->lin_d), w.v(L->lin_d), C->a.ny, C->a.nx, C->a.nb, s));
+    TRY(glide_prolong(w.dt, 2, 1, 1, wc.H(C->lin_d), w.H(L->lin_d), C->a.ny, C->a.nx, C->a.nb, s));
+    return lin_sweeps(L, c->lin_post, false, c, s);
+}
+
 int check_levels(GlideLevel* lv, int n) {
     if (!lv || n < 1) return GLIDE_E_NULL;
     for (int k = 0; k < n; k++) {
@@ -520,17 +586,38 @@ int glide_restrict_parameters(GlideLevel* levels, int n_levels, int k0, void* st
     return 0;
 }
 
+int glide_linear_setup(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, void* stream) {
+    int e = check_levels(levels, n_levels);
+    if (e) return e;
+    if (!cfg) return GLIDE_E_NULL;
+    if ((e = lin_ready(levels, n_levels))) return e;
+    return linear_setup(levels, n_levels, cfg, stream);
+}
+
+int glide_linear_vcycle(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, void* stream) {
+    int e = check_levels(levels, n_levels);
+    if (e) return e;
+    if (!cfg) return GLIDE_E_NULL;
+    if ((e = lin_ready(levels, n_levels))) return e;
+    if (cfg->lin_pre < 0 || cfg->lin_post < 0 || cfg->lin_coarse < 1) return GLIDE_E_SHAPE;
+    return lin_vcycle(levels, n_levels, 0, cfg, stream);
+}
+
 int glide_graph_create(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, int kind, void** graph_out) {
     int e = check_levels(levels, n_levels);
     if (e) return e;
     if (!cfg || !graph_out) return GLIDE_E_NULL;
+    if (kind < 0 || kind > 2) return GLIDE_E_SHAPE;
+    if (kind == 2 && ((e = lin_ready(levels, n_levels)) || cfg->lin_coarse < 1)) return e ? e : GLIDE_E_SHAPE;
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return GLIDE_E_GRAPH;
     GraphHandle* h = new GraphHandle();
     int rc = 0;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = GLIDE_E_GRAPH;
     if (!rc) {
-        rc = kind == 0 ? fascd(levels, n_levels, 0, true, cfg, s) : adjoint(levels, n_levels, 0, cfg, s);
+        rc = kind == 0   ? fascd(levels, n_levels, 0, true, cfg, s)
+             : kind == 1 ? adjoint(levels, n_levels, 0, cfg, s)
+                         : lin_vcycle(levels, n_levels, 0, cfg, s);
         cudaError_t ce = cudaStreamEndCapture(s, &h->g);
         if (!rc && ce != cudaSuccess) rc = GLIDE_E_GRAPH;
     }

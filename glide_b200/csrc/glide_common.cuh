@@ -25,7 +25,7 @@ long long launch_total();
 template <typename T> struct M;
 // FP32 exp/pow: the hardware approximations by default, as the reference's
 // --use_fast_math build of its ice kernels uses (glide/kernels.py:72);
-// -DGLIDE_FP32_ACCURATE_MATH=1 selects expf/powf.
+// -DGLIDE_FP32_ACCURATE_MATH=1 selects expf/powf and IEEE division.
 #ifndef GLIDE_FP32_ACCURATE_MATH
 #define GLIDE_FP32_ACCURATE_MATH 0
 #endif
@@ -33,9 +33,13 @@ template <> struct M<float> {
 #if GLIDE_FP32_ACCURATE_MATH
     static __device__ __forceinline__ float exp(float x) { return expf(x); }
     static __device__ __forceinline__ float pow(float x, float y) { return powf(x, y); }
+    static __device__ __forceinline__ float rcp(float x) { return 1.0f / x; }
 #else
     static __device__ __forceinline__ float exp(float x) { return __expf(x); }
     static __device__ __forceinline__ float pow(float x, float y) { return __powf(x, y); }
+    // reciprocal of the LU pivots and of the sigmoid denominator: the fast
+    // approximate division, as the reference's fast-math build divides
+    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
 #endif
     static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float abs(float x) { return fabsf(x); }
@@ -47,6 +51,7 @@ template <> struct M<double> {
     static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
     static __device__ __forceinline__ double pow(double x, double y) { return ::pow(x, y); }
     static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
     static __device__ __forceinline__ double abs(double x) { return fabs(x); }
     static __device__ __forceinline__ double copysign(double a, double b) { return ::copysign(a, b); }
     static __device__ __forceinline__ double max(double a, double b) { return fmax(a, b); }
@@ -126,7 +131,7 @@ __device__ __forceinline__ void stage(T* __restrict__ s, const T* __restrict__ g
 // --------------------------------------------------------------------------
 template <typename T> __device__ __forceinline__ T sigmoid(T z, T c) {
     T s = M<T>::min(M<T>::max(c * z, T(-20)), T(20));   // common.cu:67-70
-    return T(1) / (T(1) + M<T>::exp(-s));
+    return M<T>::rcp(T(1) + M<T>::exp(-s));
 }
 
 // Normal stress on a cell (stress.cu:43-102).  XX: 2 etaH (2 ux + vy);

@@ -394,7 +394,7 @@ template <typename T> __device__ __forceinline__ void lu5_solve_fast(T (&A)[25],
     T inv[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-        inv[k] = T(1) / A[k * 5 + k];
+        inv[k] = M<T>::rcp(A[k * 5 + k]);
 #pragma unroll
         for (int i = k + 1; i < 5; i++) {
             A[i * 5 + k] *= inv[k];
@@ -556,7 +556,7 @@ template <typename T>
 __device__ __forceinline__ void lu5_factor(T (&A)[25]) {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-        const T inv = T(1) / A[k * 5 + k];
+        const T inv = M<T>::rcp(A[k * 5 + k]);
 #pragma unroll
         for (int i = k + 1; i < 5; i++) {
             A[i * 5 + k] *= inv;
@@ -584,11 +584,12 @@ template <typename T>
 __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BLOCKS) vanka_lu_kernel(
     T* __restrict__ lu, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_H, const T* __restrict__ bed, const T* __restrict__ B, const T* __restrict__ beta,
-    const T* __restrict__ gamma, T shift, Geo g, Phys<T> p) {
+    const T* __restrict__ gamma, const T* __restrict__ act, T shift, Geo g, Phys<T> p) {
     __shared__ T s_eta[VY + 2][VX + 2];
     const int ny = g.ny, nx = g.nx;
     const int bz = blockIdx.z;
-    u += bz * g.nu(); v += bz * g.nv(); H += bz * g.nc(); f_H += bz * g.nc();
+    u += bz * g.nu(); v += bz * g.nv(); H += bz * g.nc();
+    if (act) act += bz * g.nc(); else f_H += bz * g.nc();
     bed += bz * g.nc(); B += bz * g.nc(); beta += bz * g.nc(); gamma += bz * g.nc();
     const int64_t nc = g.nc();
     lu += bz * 25 * nc;
@@ -609,8 +610,11 @@ __global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BL
     const T vt = v[ic], vb = v[int64_t(i + 1) * nx + j];
     T J[25], rr[5];
     // the momentum rows do not depend on f; the mass row's active-set switch
-    // (vanka.cu:104-113) needs the local mass residual, hence f_H
-    assemble_fast<T>(F, ul, ur, vt, vb, H[ic], T(0), T(0), T(0), T(0), f_H[ic], gamma[ic], T(1) / p.dt, p, J, rr);
+    // (vanka.cu:104-113) needs the local mass residual, hence f_H.  With a
+    // given active set (act) the switch is forced instead: a right-hand side
+    // of -/+1e30 makes H - dt r_H far below / above gamma (r is discarded).
+    const T fH = act ? (act[ic] > T(0.5) ? T(-1e30) : T(1e30)) : f_H[ic];
+    assemble_fast<T>(F, ul, ur, vt, vb, H[ic], T(0), T(0), T(0), T(0), fH, gamma[ic], T(1) / p.dt, p, J, rr);
     J[0] -= shift; J[6] -= shift; J[12] -= shift; J[18] -= shift; J[24] += shift;  // vanka.cu:406-410
     lu5_factor(J);
 #pragma unroll
@@ -834,9 +838,10 @@ template <typename T>
 int launch_vanka_lu(const GlideLevelArgs* a, const void* f_H, void* lu, double shift, cudaStream_t s) {
     Geo g{a->ny, a->nx, a->nb};
     Phys<T> p = make_phys<T>(a->params, a->dx, a->dt);
+    // f_H null: the active set is the level's mask (glide_vanka_lu_masked)
     glide::count_launch(), vanka_lu_kernel<T><<<cell_grid(g), VNT, 0, s>>>(
         (T*)lu, (const T*)a->u, (const T*)a->v, (const T*)a->H, (const T*)f_H, (const T*)a->bed, (const T*)a->B,
-        (const T*)a->beta, (const T*)a->gamma, T(shift), g, p);
+        (const T*)a->beta, (const T*)a->gamma, f_H ? nullptr : (const T*)a->mask, T(shift), g, p);
     return (int)cudaGetLastError();
 }
 

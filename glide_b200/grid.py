@@ -119,6 +119,30 @@ class Grid:
             L.norm_parts = self._norm_parts.data_ptr()
         return L
 
+    def newton_buffers(self):
+        """Buffers of the linear multigrid of the Newton-Krylov finishing
+        solver (allocated on first use): local factors, right-hand side,
+        linear residual, correction, residual at the linearisation state, and
+        the active set (kept apart from ``mask``, which the FAS cycle reads)."""
+        if getattr(self, "_nk", None) is None:
+            self._nk = {"lu": torch.zeros(25 * self.nb * self.nh, dtype=self.dtype, device=self.device),
+                        "lin_rhs": self._vec(), "lin_rho": self._vec(), "lin_d": self._vec(), "r_raw": self._vec(),
+                        "mask": self._cells()}
+        return self._nk
+
+    def newton_level(self, gl_sigmoid_c):
+        """native_level() with the Newton-Krylov buffers attached, the active
+        set in its own mask and the exact grounding-line derivatives in the
+        Jacobian (they change J, not the residual)."""
+        L = self.native_level()
+        b = self.newton_buffers()
+        L.lu, L.lin_rhs, L.lin_rho = b["lu"].data_ptr(), b["lin_rhs"].data_ptr(), b["lin_rho"].data_ptr()
+        L.lin_d, L.r_raw = b["lin_d"].data_ptr(), b["r_raw"].data_ptr()
+        L.a.mask = b["mask"].data_ptr()
+        L.a.params.gl_derivatives = 1
+        L.a.params.gl_sigmoid_c = float(gl_sigmoid_c)
+        return L
+
     def _s(self):
         return N.stream_handle()
 

@@ -54,6 +54,31 @@ def _as_tensor(x, dtype, device, shape=None):
     return t
 
 
+class _NativeProducts:
+    """The two vector products of the Anderson step on the library's kernels:
+    dot products of stored rows with one vector (FP64 accumulation, fixed
+    order) and a linear combination of stored rows."""
+
+    def __init__(self, n, dtype, device):
+        self.lib = N.load()
+        self.n, self.code = int(n), N.dtype_code(dtype)
+        self.parts = torch.zeros(self.lib.glide_dots_parts(self.n) * 32, dtype=torch.float64, device=device)
+        self.out = torch.zeros(32, dtype=torch.float64, device=device)
+        self.coef = torch.zeros(32, dtype=torch.float64, device=device)
+
+    def dots(self, rows, w):
+        k = rows.shape[0]
+        N.check(self.lib.glide_dots(self.code, self.n, k, rows.data_ptr(), self.n, w.data_ptr(), self.out.data_ptr(),
+                                    self.parts.data_ptr(), N.stream_handle()), "dots")
+        return self.out[:k].cpu().numpy()
+
+    def combine(self, rows, coef, out):
+        k = rows.shape[0]
+        self.coef[:k].copy_(torch.as_tensor(coef, dtype=torch.float64))
+        N.check(self.lib.glide_combine(self.code, self.n, k, rows.data_ptr(), self.n, self.coef.data_ptr(), 1.0,
+                                       out.data_ptr(), 0.0, N.stream_handle()), "combine")
+
+
 class _Anderson:
     """Anderson acceleration (depth m) of the velocity over finishing blocks.
 
@@ -61,17 +86,19 @@ class _Anderson:
     dF, dG the differences of consecutive f and G, the next state is
     G_k - dG gam, gam = argmin |f_k - dF gam| (normal equations, Tikhonov
     1e-12 trace).  The last m + 1 pairs live in preallocated ring buffers; each
-    block adds one matrix-vector product for the new f's dot products (the
-    small Gram matrix is kept on the host) and one for the combination, so no
-    history is stacked or copied.
+    block adds one multi-dot pass for the new f's dot products (the small Gram
+    matrix is kept on the host) and one linear combination, so no history is
+    stacked or copied.  ``products`` supplies those two device products
+    (default: the library's kernels).
     """
 
-    def __init__(self, m, n, dtype, device):
+    def __init__(self, m, n, dtype, device, products=None):
         self.m = int(m)
         self.F = torch.zeros(self.m + 1, n, dtype=dtype, device=device)
         self.G = torch.zeros(self.m + 1, n, dtype=dtype, device=device)
         self.gram = np.zeros((self.m + 1, self.m + 1))
         self.order = []
+        self.products = products if products is not None else _NativeProducts(n, dtype, device)
 
     def reset(self):
         self.order = []
@@ -86,7 +113,7 @@ class _Anderson:
         self.order.append(slot)
         torch.sub(x, x_before, out=self.F[slot])
         self.G[slot].copy_(x)
-        dots = torch.mv(self.F, self.F[slot]).cpu().numpy()
+        dots = self.products.dots(self.F, self.F[slot])
         self.gram[slot, :] = dots
         self.gram[:, slot] = dots
         k = len(self.order)
@@ -109,7 +136,7 @@ class _Anderson:
         c[-1] += 1.0
         full = np.zeros(self.m + 1)
         full[self.order] = c
-        torch.mv(self.G.T, torch.as_tensor(full, dtype=self.G.dtype, device=self.G.device), out=x)
+        self.products.combine(self.G, full, x)
 
 
 class IcePhysics:
@@ -120,7 +147,9 @@ class IcePhysics:
                  settings: SolverSettings | None = None, batch=1, use_graphs=True, guess_min_reduction=10.0,
                  stall_factor=0.5, finish_block=20, finish_anderson=0, finish_fp32=False, finish_newton=None,
                  finish_step=None, finish_linear=False, finish_patience=3,
-                 finish_fas_until=math.inf, finish_fas_patience=10):
+                 finish_fas_until=math.inf, finish_fas_patience=10, newton=False, newton_start=1e-3,
+                 newton_max_steps=8, newton_rtol=1e-2, newton_krylov=20, newton_min_gain=1.0,
+                 newton_local=0, newton_after=0):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -148,6 +177,17 @@ class IcePhysics:
         self.finish_patience = int(finish_patience)
         self.finish_fas_until = float(finish_fas_until)
         self.finish_fas_patience = int(finish_fas_patience)
+        if newton and precision != "mixed":
+            raise ValueError('newton=True needs precision="mixed" (FP32 corrections of an FP64 state)')
+        self.newton = bool(newton)
+        self.newton_start = float(newton_start)
+        self.newton_max_steps = int(newton_max_steps)
+        self.newton_rtol = float(newton_rtol)
+        self.newton_krylov = int(newton_krylov)
+        self.newton_min_gain = float(newton_min_gain)
+        self.newton_local = int(newton_local)
+        self.newton_after = int(newton_after)
+        self._nk = None
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
         self.dtype = _PRECISIONS[precision]
@@ -371,6 +411,9 @@ class IcePhysics:
             if tol is not None and finish and rel > self.stall_factor * prev:
                 stalled = True
                 break
+            if tol is not None and finish and self.newton and self.newton_after == 0 and rel <= self.newton_start:
+                stalled = True   # close enough for the Newton-Krylov finish
+                break
             prev = rel
         if tol is not None and finish and rel > tol and (stalled or k >= n_max):
             rel = self._finish(r0, tol, max_finish_sweeps, hist, info, verbose, rel)
@@ -439,7 +482,26 @@ class IcePhysics:
         blocks = {"fp32": 0, "fp64": 0}
         info["finish_blocks"] = blocks
         fas_until = self.finish_fas_until
+        nk_last = math.inf   # |r|/|r0| at the last Newton-Krylov attempt
+        nk_tries = 0
         while done < max_sweeps and rel > tol:
+            if (self.newton and rel <= self.newton_start and rel < 0.5 * nk_last and nk_tries < 3 and
+                    done >= self.newton_after):
+                # Newton-Krylov from here; a failed attempt falls back to the blocks below, and a
+                # new attempt follows once they have halved the residual
+                nk_tries += 1
+                rel = self._newton_krylov().solve(r0, tol, rel, hist, info, max_steps=self.newton_max_steps,
+                                                  rtol=self.newton_rtol, min_gain=self.newton_min_gain,
+                                                  local_rounds=self.newton_local)
+                nk_last = rel
+                if rel < best:
+                    best = rel
+                    good.copy_(g.U)
+                    since_best = 0
+                if aa is not None:
+                    aa.reset()
+                prev = rel
+                continue
             if m > 0:
                 x0.copy_(g.U[:nU])
             blocks["fp32" if use32 else "fp64"] += 1
@@ -512,6 +574,12 @@ class IcePhysics:
             prev = rel
         info["finish_sweeps"] = done
         return rel
+
+    def _newton_krylov(self):
+        from .newton import NewtonKrylov
+        if self._nk is None:
+            self._nk = NewtonKrylov(self, m=self.newton_krylov)
+        return self._nk
 
     def _finish_local(self):
         """Local Newton iterations and step fraction of the finishing sweeps
@@ -703,6 +771,8 @@ class IcePhysics:
 
     def release_graphs(self):
         self._graphs.clear()
+        if self._nk is not None:
+            self._nk.release()
 
 
 # ---------------------------------------------------------------------------

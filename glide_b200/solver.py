@@ -35,6 +35,12 @@ class SolverSettings:
     newton_step: float = 0.25  # fraction of each local Newton step (relaxation_factor, glide/cuda/vanka.cu:416)
     coarse_line_search: bool = False  # finest-level step on the coarse correction (reference: full step)
     pivoted_lu: bool = False   # row-pivoted local solves (glide/cuda/common.cu:180-233; unused by the reference)
+    # linear V-cycle of the Newton-Krylov finishing solver (no counterpart in the reference)
+    lin_pre: int = 2           # linear Vanka sweeps before the coarse correction
+    lin_post: int = 2          # ... and after it
+    lin_coarse: int = 20       # linear sweeps on the coarsest level
+    lin_omega: float = 0.5     # damping of each linear sweep
+    lin_shift: float = 0.0     # diagonal shift of the local factors
 
     def native(self, thklim) -> N.SolverConfig:
         c = N.SolverConfig()
@@ -48,6 +54,8 @@ class SolverSettings:
         c.newton_step = float(self.newton_step)
         c.coarse_line_search = int(self.coarse_line_search)
         c.pivoted_lu = int(self.pivoted_lu)
+        c.lin_pre, c.lin_post, c.lin_coarse = int(self.lin_pre), int(self.lin_post), int(self.lin_coarse)
+        c.lin_omega, c.lin_shift = float(self.lin_omega), float(self.lin_shift)
         return c
 
 

@@ -111,9 +111,12 @@ int glide_vanka_sweeps_ex(const GlideLevelArgs* a, const void* f_u, const void* 
  * 10 MiB device array inside the library (glide_noalloc_scratch_bytes()),
  * enough for nb*ny*nx <= 262144 cells in FP64 or 524288 in FP32; larger
  * problems return GLIDE_E_TOO_LARGE.  The first call on a device (with that
- * device current) looks up the array's device address; make it before any
- * stream capture.  All calls share the array, so calls that overlap on the
- * GPU race and must be ordered by the caller.  Allocates nothing. */
+ * device current) looks up the array's device address and keeps it for that
+ * CUDA context; a call in a new context of the device (after
+ * cudaDeviceReset) looks it up again.  Make the first call, and the first
+ * after a reset, before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU race and must be ordered by the caller.
+ * Allocates nothing. */
 int glide_vanka_sweeps_noalloc(const GlideLevelArgs* a, const void* f_u, const void* f_v, const void* f_H, int n_iter,
                                int n_newton, double omega, double shift, const int* flags, const int* any_active,
                                void* stream);
@@ -180,6 +183,13 @@ typedef struct GlideLevel {
     void* ls_tmp;           /* one state vector (like U) */
     double* ls_norms;       /* 3 * GLIDE_LS_CANDIDATES + 1 doubles */
     double* norm_parts;     /* 3 * glide_norm_parts(max(nu, nc) * nb) doubles */
+    /* linear multigrid of the Newton-Krylov finishing solver (may be null when
+       glide_linear_setup / glide_linear_vcycle are not used) */
+    void* lu;               /* 25 * nc * nb: local Vanka factors at the level's state */
+    void* lin_rhs;          /* like U: right-hand side g of J d = -g */
+    void* lin_rho;          /* like U: linear residual g + J d */
+    void* lin_d;            /* like U: correction d */
+    void* r_raw;            /* like U: residual at the linearisation state (active-set test) */
 } GlideLevel;
 
 /* Step sizes tried by the coarse-correction line search, best first on ties. */
@@ -200,6 +210,11 @@ typedef struct GlideSolverConfig {
     int coarse_line_search; /* 1: on the finest level, U = U_pre + a * P(U_c - w_c) with a in
                                {1, 1/2, 1/4, 0} minimising the residual norm (chosen on the
                                device); 0: a = 1 (reference) */
+    /* linear V-cycle of the Newton-Krylov finishing solver (glide_linear_vcycle) */
+    int lin_pre, lin_post;  /* linear Vanka sweeps before / after the coarse correction */
+    int lin_coarse;         /* linear sweeps on the coarsest level */
+    double lin_omega;       /* damping of each linear sweep */
+    double lin_shift;       /* diagonal shift of the local factors (0: the local Jacobian) */
 } GlideSolverConfig;
 
 /* One FASCD V-cycle from level k0 (finest=1 sets w=U, chi=gamma-H first). */
@@ -209,7 +224,45 @@ int glide_adjoint_vcycle(GlideLevel* levels, int n_levels, int k0, const GlideSo
 /* restrict bed, B, beta, H_prev, smb from every level to its child (glide/solver.py:53-68) */
 int glide_restrict_parameters(GlideLevel* levels, int n_levels, int k0, void* stream);
 
-/* CUDA graphs of whole V-cycles.  kind: 0 = FASCD (finest), 1 = adjoint.
+/* Newton-Krylov finishing solver (no counterpart in the reference, which runs
+ * a fixed number of FAS V-cycles): a linear multigrid V-cycle for the
+ * correction d of J(U) d = -g, with the additive linear Vanka sweep as the
+ * smoother on every level and each coarse level linearised at the restricted
+ * state.  glide_linear_setup expects level 0's state, mask (the active set),
+ * lin_rhs (g) and r_raw (the residual at U) to be set; it restricts the state
+ * and r_raw down the hierarchy, sets each coarse level's active set from
+ * H - dt r_H <= gamma (gamma = thklim) and factors every level's local
+ * matrices (glide_vanka_lu_masked).  glide_linear_vcycle then writes level
+ * 0's lin_d from its lin_rhs (graph-capturable, no host synchronisation). */
+int glide_linear_setup(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, void* stream);
+int glide_linear_vcycle(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, void* stream);
+/* glide_vanka_lu with the active set given by a->mask (1 = the cell's mass
+ * row is the constraint H = gamma) instead of the local residual test. */
+int glide_vanka_lu_masked(const GlideLevelArgs* a, void* lu, double shift, void* stream);
+/* Newton step helpers (no counterpart in the reference).  glide_newton_rhs:
+ * from the FP64 residual r (monolithic, faces then cells) of the FP64 level
+ * a64, the active set H - dt r_H <= gamma into mask32 (cells) and the FP32
+ * right-hand side rhs32 (r with active rows replaced by H - gamma) and
+ * rraw32 = fl32(r).  glide_newton_update: U64 = base64 + alpha * fl64(d32)
+ * with H kept >= gamma.  glide_active_mask: mask = (H - dt r_H <= gamma). */
+int glide_newton_rhs(const GlideLevelArgs* a64, const void* r64, void* rhs32, void* rraw32, void* mask32,
+                     void* stream);
+int glide_newton_update(const GlideLevelArgs* a64, void* U64, const void* base64, const void* d32, double alpha,
+                        void* stream);
+int glide_active_mask(const GlideLevelArgs* a, const void* r_H, void* mask, void* stream);
+/* out[i] = sum_j V[i*ldv + j] * w[j], i < k <= 32, FP64 accumulation in a fixed
+ * order (deterministic); out: k device doubles; parts: glide_dots_parts(n) * k
+ * doubles of scratch.  glide_combine: out = beta * out + alpha * sum_i coef[i]
+ * V[i] (coef: k device doubles; beta = 0 does not read out).  The Krylov and
+ * Anderson steps of the tolerance solver. */
+int glide_dots(int dtype, int64_t n, int k, const void* V, int64_t ldv, const void* w, double* out, double* parts,
+               void* stream);
+int glide_dots_parts(int64_t n);
+int glide_combine(int dtype, int64_t n, int k, const void* V, int64_t ldv, const double* coef, double alpha,
+                  void* out, double beta, void* stream);
+
+/* CUDA graphs of whole V-cycles.  kind: 0 = FASCD (finest), 1 = adjoint,
+ * 2 = linear V-cycle (glide_linear_vcycle).
  * The graph keeps the device pointers it was built with. */
 int glide_graph_create(GlideLevel* levels, int n_levels, const GlideSolverConfig* cfg, int kind, void** graph_out);
 int glide_graph_launch(void* graph, void* stream);

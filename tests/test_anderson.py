@@ -1,9 +1,19 @@
 """Anderson acceleration of the finishing blocks (glide_b200.physics._Anderson)
-on CPU: on a linear contraction x -> A x + b it reproduces the textbook
-stacked-history formulation step by step and converges far faster than the
-plain iteration."""
+on CPU: on a linear contraction x -> A x + b its host-side bookkeeping
+reproduces the textbook stacked-history formulation step by step and
+converges far faster than the plain iteration.  The two device products
+(multi-dot, combination; the library's kernels on the GPU, checked in
+tests/test_gpu_krylov.py) are replaced here by plain torch products."""
 import numpy as np
 import torch
+
+
+class _TorchProducts:
+    def dots(self, rows, w):
+        return (rows @ w).numpy()
+
+    def combine(self, rows, coef, out):
+        out.copy_(rows.T @ torch.as_tensor(coef, dtype=rows.dtype))
 
 
 def _reference_aa(g, x0, m, iters):
@@ -36,7 +46,7 @@ def test_anderson_matches_reference_and_accelerates():
     g = lambda x: A @ x + b
     x_star = np.linalg.solve(np.eye(n) - A, b)
     ref = _reference_aa(g, np.zeros(n), 3, 25)
-    aa = _Anderson(3, n, torch.float64, "cpu")
+    aa = _Anderson(3, n, torch.float64, "cpu", products=_TorchProducts())
     x = torch.zeros(n, dtype=torch.float64)
     before = torch.empty_like(x)
     for k in range(25):
