@@ -46,6 +46,7 @@ DX = 1000.0
 LEVELS = 6
 DT = 10.0
 TOL = 1e-6
+MAX_FINISH = 20000   # finishing-sweep budget of a step: every timed step must reach TOL
 
 
 def parse():
@@ -64,6 +65,9 @@ def parse():
     ap.add_argument("--kernels", action="store_true",
                     help="per-kernel GB/s table on the marine configuration instead of the metric line")
     ap.add_argument("--kernels-n", type=int, default=4096, help="grid size of the --kernels table")
+    ap.add_argument("--kernels-compare", action="store_true",
+                    help="per-call times of the hot kernels at 1024^2 and 4096^2 (with --impl reference: the "
+                         "reference's own kernels on the same state)")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying CUDA graphs (for profiler runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -194,7 +198,14 @@ def fast_settings():
 
 
 FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0, finish_linear="after",
-               finish_fas_until=2e-4, finish_fas_patience=8)
+               finish_fas_until=2e-4, finish_fas_patience=8,
+               newton=True, newton_start=1e-2, newton_after=200, newton_min_gain=4.0, newton_local=2,
+               newton_max_steps=6)
+# the fast path's smoother and finishing rule in FP64 (no FP32 correction stages)
+FP64_FAST_KW = dict(finish_anderson=3, finish_newton=2, finish_step=1.0)
+FAST_PATH = ("mixed FAS, full-step local Newton x2, finishing sweeps FP32 (FAS form, then linearised) / FP64 + "
+             "Anderson(3); after 200 sweeps a Newton-Krylov finish (FGMRES, linear multigrid V-cycle "
+             "preconditioner) while its steps gain >= 4x")
 
 
 def make_cases(n, seeds):
@@ -219,7 +230,7 @@ class Runner:
         d = dict(bed=case.bed, H=case.thickness, B=case.B, beta=case.beta, smb=case.smb)
         return {k: t.as_tensor(v, dtype=self.ph.dtype, device="cuda") for k, v in d.items()}
 
-    def step(self, dev, tol=None):
+    def step(self, dev, tol=None, max_finish_sweeps=MAX_FINISH):
         ph = self.ph
         ph.set_geometry(dev["bed"], dev["H"])
         ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
@@ -227,7 +238,8 @@ class Runner:
         guess = None
         if self.guess_model is not None:
             guess = self.guess_model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"])
-        ph.forward(DT, tol=TOL if tol is None else tol, max_vcycles=self.max_vcycles, guess=guess)
+        ph.forward(DT, tol=TOL if tol is None else tol, max_vcycles=self.max_vcycles, guess=guess,
+                   max_finish_sweeps=max_finish_sweeps)
         return dict(ph.last_info)
 
 
@@ -253,10 +265,12 @@ def launches(runner):
 
 
 def time_steps(runner, devs, warmup, steps, world, flush, keep=None):
-    """W untimed and K timed steps on fresh geometries; with ``keep`` (a list)
-    each timed step's FP64 state is copied there after its timed region."""
+    """W untimed and K timed steps on fresh geometries.  Returns the total
+    time, the per-step times (ms) and the solver records; with ``keep`` (a
+    list) each timed step's FP64 state is copied to the host there, after its
+    timed region."""
     import torch
-    infos = []
+    infos, step_ms = [], []
     for k in range(warmup):
         runner.step(devs[k % len(devs)])
     torch.cuda.synchronize()
@@ -274,9 +288,79 @@ def time_steps(runner, devs, warmup, steps, world, flush, keep=None):
         torch.cuda.synchronize()
         runner.launches += launches(runner) - l0
         total += a.elapsed_time(b) / 1e3
+        step_ms.append(round(a.elapsed_time(b), 2))
         if keep is not None:
-            keep.append(runner.ph.grid.U.detach().to(torch.float64).clone())
-    return total, infos
+            keep.append(runner.ph.grid.U.detach().to(torch.float64).cpu())
+    return total, step_ms, infos
+
+
+def host_inputs(cases):
+    """Pinned FP64 host copies of every case's inputs (the end-to-end arm's source)."""
+    import numpy as np
+    import torch
+    return [{k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float64).pin_memory()
+             for k, v in (("bed", c.bed), ("H", c.thickness), ("B", c.B), ("beta", c.beta), ("smb", c.smb))}
+            for c in cases]
+
+
+def e2e_step(ph, d, out_u, out_v, max_vcycles):
+    """One step through the public API from host buffers: inputs copied to
+    the device, the solve, (u, v) copied back."""
+    dev = {key: val.to("cuda", non_blocking=True) for key, val in d.items()}
+    ph.set_geometry(dev["bed"], dev["H"])
+    ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
+    ph.reset_solution()
+    u, v, H = ph.forward(DT, tol=TOL, max_vcycles=max_vcycles, max_finish_sweeps=MAX_FINISH)
+    out_u.copy_(u, non_blocking=True)
+    out_v.copy_(v, non_blocking=True)
+
+
+def time_fast_and_e2e(fast, fdev, host, args, world, flush, n, keep=None):
+    """The fast path timed two ways on the same geometries, step by step in
+    alternation (so that both see the same clocks, warm state and sampler):
+    ``value`` with inputs already resident in HBM, ``e2e`` through IcePhysics
+    from pinned host buffers with the host<->device copies in its timed
+    region.  Returns both totals, per-step times, solver records, launches
+    and the bytes copied per e2e step."""
+    import torch
+    out_u = torch.empty((n, n + 1), dtype=torch.float64).pin_memory()
+    out_v = torch.empty((n + 1, n), dtype=torch.float64).pin_memory()
+    ph = fast.ph
+    for k in range(args.warmup):
+        fast.step(fdev[k])
+        e2e_step(ph, host[k], out_u, out_v, args.max_vcycles)
+    torch.cuda.synchronize()
+    t_val = t_e2e = 0.0
+    ms_val, ms_e2e, infos = [], [], []
+    fast.launches = 0
+    for k in range(args.steps):
+        i = args.warmup + k
+        for arm in ("value", "e2e"):
+            flush_l2(flush)
+            barrier(world)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = launches(fast)
+            a.record()
+            if arm == "value":
+                infos.append(fast.step(fdev[i]))
+            else:
+                e2e_step(ph, host[i], out_u, out_v, args.max_vcycles)
+            b.record()
+            torch.cuda.synchronize()
+            dt = a.elapsed_time(b)
+            if arm == "value":
+                fast.launches += launches(fast) - l0
+                t_val += dt / 1e3
+                ms_val.append(round(dt, 2))
+                if keep is not None:
+                    keep.append(ph.grid.U.detach().to(torch.float64).cpu())
+            else:
+                t_e2e += dt / 1e3
+                ms_e2e.append(round(dt, 2))
+    h2d = sum(t.numel() * t.element_size() for t in host[0].values())
+    d2h = out_u.numel() * 8 + out_v.numel() * 8
+    return t_val, t_e2e, ms_val, ms_e2e, infos, h2d, d2h
 
 
 def kernel_timings(runner, launches=20):
@@ -375,7 +459,7 @@ def warm_start(runner, case, args, world, flush):
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles)
+        ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles, max_finish_sweeps=MAX_FINISH)
         b.record()
         torch.cuda.synchronize()
         if k >= args.warmup:
@@ -389,42 +473,24 @@ def warm_start(runner, case, args, world, flush):
             "series": f"steps {args.warmup + 1}..{args.warmup + args.steps} of one geometry, dt={DT:g} a"}
 
 
-def end_to_end(fast, cases, args, world, flush, n):
-    """Steps/s through IcePhysics with host (pinned) inputs: every step copies
-    its inputs host->device and reads (u, v) back inside the timed region."""
-    import numpy as np
-    import torch
-    host = []
-    for c in cases:
-        d = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float64).pin_memory()
-             for k, v in (("bed", c.bed), ("H", c.thickness), ("B", c.B), ("beta", c.beta), ("smb", c.smb))}
-        host.append(d)
-    out_u = torch.empty((n, n + 1), dtype=torch.float64).pin_memory()
-    out_v = torch.empty((n + 1, n), dtype=torch.float64).pin_memory()
-    ph = fast.ph
-    tot = 0.0
-    for k in range(args.warmup + args.steps):
-        d = host[k]
-        flush_l2(flush)
-        barrier(world)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        dev = {key: val.to("cuda", non_blocking=True) for key, val in d.items()}
-        ph.set_geometry(dev["bed"], dev["H"])
-        ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
-        ph.reset_solution()
-        u, v, H = ph.forward(DT, tol=TOL, max_vcycles=args.max_vcycles)
-        out_u.copy_(u, non_blocking=True)
-        out_v.copy_(v, non_blocking=True)
-        b.record()
-        torch.cuda.synchronize()
-        if k >= args.warmup:
-            tot += a.elapsed_time(b) / 1e3
-    h2d = sum(t.numel() * t.element_size() for t in host[0].values())
-    d2h = out_u.numel() * 8 + out_v.numel() * 8
-    tot = max_over_ranks(tot, world)
-    return world * args.steps / tot, h2d, d2h
+def branch_report(sols_a, sols_b, seeds, n, threshold=1e-3):
+    """Geometries whose two answers differ by more than ``threshold``
+    (relative 2-norm of u): where they differ (faces / cells whose value
+    differs by more than ``threshold`` times the field's largest magnitude)."""
+    nu, nv = n * (n + 1), (n + 1) * n
+    out = []
+    for a, b, seed in zip(sols_a, sols_b, seeds):
+        du = float((a[:nu] - b[:nu]).norm() / b[:nu].norm().clamp_min(1e-300))
+        if du <= threshold:
+            continue
+        rec = {"seed": seed, "u_rel": du}
+        for name, sl in (("u", slice(0, nu)), ("v", slice(nu, nu + nv)), ("H", slice(nu + nv, None))):
+            d = (a[sl] - b[sl]).abs()
+            scale = float(b[sl].abs().max())
+            rec[f"{name}_points_differing"] = int((d > threshold * scale).sum())
+            rec[f"{name}_max_abs_diff"] = float(d.max())
+        out.append(rec)
+    return out
 
 
 def run_ours(args):
@@ -433,6 +499,7 @@ def run_ours(args):
     n = args.n
     seeds = rank_seeds(rank, args.warmup + args.steps)
     cases = make_cases(n, seeds)
+    timed_seeds = seeds[args.warmup:]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 
     guess_model = None
@@ -444,55 +511,76 @@ def run_ours(args):
     fast = Runner(n, "mixed", None, args.max_vcycles, fast_settings(), use_graphs=not args.eager, **FAST_KW)
     fdev = [fast.load_device(c) for c in cases]
 
+    # the clock sampler runs over every timed arm
     sampler = ClockSampler(local)
     if not args.no_clocks:
         sampler.start()
-    sol_fast, sol_guess, sol_plain = [], [], []
-    t_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush, sol_fast)
-    sampler.stop()
+    sols = {"fast": [], "learned_guess": [], "fp64_fast_smoother": [], "plain_fp64_fas": []}
+    e2e_val, h2d, d2h, ms_e2e = None, 0, 0, []
+    if args.no_e2e:
+        t_fast, ms_fast, info_fast = time_steps(fast, fdev, args.warmup, args.steps, world, flush, sols["fast"])
+    else:
+        host = host_inputs(cases)
+        t_fast, t_e2e, ms_fast, ms_e2e, info_fast, h2d, d2h = time_fast_and_e2e(fast, fdev, host, args, world,
+                                                                                 flush, n, sols["fast"])
+        e2e_val = world * args.steps / max_over_ranks(t_e2e, world)
+        del host
+    fast_launches = fast.launches
     t_fast = max_over_ranks(t_fast, world)
     value = world * args.steps / t_fast
-    fast_launches = fast.launches
 
-    guess_val, info_guess = None, []
+    arms = {}
     if guess_model is not None and not args.no_guess:
         fast.guess_model = guess_model
-        t_guess, info_guess = time_steps(fast, fdev, args.warmup, args.steps, world, flush, sol_guess)
-        t_guess = max_over_ranks(t_guess, world)
-        guess_val = world * args.steps / t_guess
+        t, ms, infos = time_steps(fast, fdev, args.warmup, args.steps, world, flush, sols["learned_guess"])
+        arms["learned_guess"] = (world * args.steps / max_over_ranks(t, world), ms, infos)
         fast.guess_model = None
-
-    plain_val, info_plain = None, []
     if not args.no_plain:
+        # same smoother and finishing rule as the fast path, all in FP64: the precision gain alone
+        f64 = Runner(n, "fp64", None, args.max_vcycles, fast_settings(), use_graphs=not args.eager, **FP64_FAST_KW)
+        t, ms, infos = time_steps(f64, [f64.load_device(c) for c in cases], args.warmup, args.steps, world, flush,
+                                  sols["fp64_fast_smoother"])
+        arms["fp64_fast_smoother"] = (world * args.steps / max_over_ranks(t, world), ms, infos)
+        del f64
+        # the reference's smoother constants in FP64: the smoother gain on top
         plain = Runner(n, "fp64", None, args.max_vcycles, use_graphs=not args.eager)
-        pdev = [plain.load_device(c) for c in cases]
-        t_plain, info_plain = time_steps(plain, pdev, args.warmup, args.steps, world, flush, sol_plain)
-        t_plain = max_over_ranks(t_plain, world)
-        plain_val = world * args.steps / t_plain
-        del plain, pdev
+        t, ms, infos = time_steps(plain, [plain.load_device(c) for c in cases], args.warmup, args.steps, world,
+                                  flush, sols["plain_fp64_fas"])
+        arms["plain_fp64_fas"] = (world * args.steps / max_over_ranks(t, world), ms, infos)
+        del plain
+        torch.cuda.empty_cache()
+    sampler.stop()
+
     # accuracy of the fast path's answers: against the same solve continued to
     # TOL_TIGHT (its residual is evaluated in FP64, so that state solves the
     # FP64 discrete equations to TOL_TIGHT, on the same solution branch)
     sol_tight, rel_tight = [], []
     for k in range(args.steps):
         rel_tight.append(fast.step(fdev[args.warmup + k], tol=TOL_TIGHT)["rel_residual"])
-        sol_tight.append(fast.ph.grid.U.detach().to(torch.float64).clone())
-    err = {"fast": solution_error(sol_fast, sol_tight, n),
+        sol_tight.append(fast.ph.grid.U.detach().to(torch.float64).cpu())
+    kept = [k for k, r in enumerate(rel_tight) if r is not None and r <= TOL_TIGHT]
+    err = {"fast": solution_error([sols["fast"][k] for k in kept], [sol_tight[k] for k in kept], n) if kept else None,
            "reference_solution": f"the same solve continued to {TOL_TIGHT:g} relative residual (FP64 residual)",
-           "reference_rel_residual_max": max(rel_tight),
-           "note": "largest relative 2-norm difference per field over the timed steps"}
-    if sol_plain:
-        err["fast_vs_plain_fp64"] = solution_error(sol_fast, sol_plain, n)
-        if sol_guess:
-            err["learned_guess_vs_plain_fp64"] = solution_error(sol_guess, sol_plain, n)
-        err["vs_plain_note"] = ("the implicit step can have more than one solution near floating margins "
-                                "(calving and the grounding sigmoid make the mass balance bistable); the paths "
-                                "may converge to different ones, so these differences do not shrink with the "
-                                "tolerance and are not precision errors")
-    del sol_fast, sol_guess, sol_plain, sol_tight
+           "reference_rel_residual": rel_tight,
+           "reference_rel_residual_max": max(rel_tight[k] for k in kept) if kept else None,
+           "dropped_seeds": [timed_seeds[k] for k in range(args.steps) if k not in kept],
+           "note": "largest relative 2-norm difference per field over the timed steps whose reference reached "
+                   f"{TOL_TIGHT:g}; dropped_seeds lists those that did not"}
+    if sols["plain_fp64_fas"]:
+        err["fast_vs_plain_fp64"] = solution_error(sols["fast"], sols["plain_fp64_fas"], n)
+        if sols["learned_guess"]:
+            err["learned_guess_vs_plain_fp64"] = solution_error(sols["learned_guess"], sols["plain_fp64_fas"], n)
+        err["branches"] = branch_report(sols["fast"], sols["plain_fp64_fas"], timed_seeds, n)
+        err["branches_note"] = ("geometries where the fast and plain answers differ by more than 1e-3 in u; "
+                                "oracle_rel_residual shows both answers solve the FP64 equations to the tolerance")
 
-    # end to end through the public API: host (pinned) inputs, H2D each step, D2H of u, v
-    e2e_val, h2d, d2h = (None, 0, 0) if args.no_e2e else end_to_end(fast, cases, args, world, flush, n)
+    # end-of-run checks on rank 0 at N=1: the CPU baseline and the oracle's
+    # FP64 residual of every arm's answers (the oracle as the checker, untimed)
+    cpu, oracle_rel = None, None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(cases[0], arms.get("plain_fp64_fas", (None, None, []))[2])
+        oracle_rel = oracle_check(cases[args.warmup:], {**sols, "tight": sol_tight})
+    del sols, sol_tight
 
     # dominant-kernel roofline (Vanka cell kernel, fine level of the FP32 hierarchy)
     roof = roofline(kernel_timings(fast), n)
@@ -505,16 +593,27 @@ def run_ours(args):
             warm["plain_fp64_fas"] = warm_start(plain_w, cases[0], args, world, flush)
             del plain_w
 
-    cpu = None
-    if rank == 0 and not args.no_cpu:
-        cpu = cpu_baseline(cases[0], info_plain)
-
-    def arm(val, infos):
-        return {"value": val, "unit": "steps/s", "vcycles_per_step": [i.get("vcycles") for i in infos],
-                "finish_sweeps_per_step": [i.get("finish_sweeps") for i in infos],
-                "rel_residual_reached": [i.get("rel_residual") for i in infos]}
+    def arm(val, ms, infos, name):
+        out = {"value": val, "unit": "steps/s", "step_ms": ms,
+               "vcycles_per_step": [i.get("vcycles") for i in infos],
+               "finish_sweeps_per_step": [i.get("finish_sweeps") for i in infos],
+               "rel_residual_reached": [i.get("rel_residual") for i in infos]}
+        if any("newton_steps" in i for i in infos):
+            out["newton_steps_per_step"] = [i.get("newton_steps", 0) for i in infos]
+            out["krylov_its_per_step"] = [i.get("krylov_its", 0) for i in infos]
+        if oracle_rel is not None and name in oracle_rel:
+            out["oracle_rel_residual"] = oracle_rel[name]
+        return out
 
     if rank == 0:
+        fast_arm = arm(value, ms_fast, info_fast, "fast")
+        if oracle_rel is not None and "tight" in oracle_rel:
+            err["reference_oracle_rel_residual"] = oracle_rel["tight"]
+        summary = {"fast": value, "e2e": e2e_val}
+        for name in ("learned_guess", "fp64_fast_smoother", "plain_fp64_fas"):
+            summary[name] = arms[name][0] if name in arms else None
+        if oracle_rel is not None:
+            summary["oracle_rel_residual_max"] = {k: max(v) for k, v in oracle_rel.items() if v}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_fast / args.steps, "higher_is_better": True,
@@ -522,25 +621,48 @@ def run_ours(args):
             "data": "synthetic (seeded grounded-dome geometries, fresh per step)",
             "config": {"workload": f"forward step to {TOL:g} rel. residual, {n}x{n}, dx={DX * 1024 / n:g} m, "
                                    f"{LEVELS} levels, dt={DT:g} a, fresh geometry per step",
-                       "path": "mixed FAS, full-step local Newton x2, finishing sweeps FP32 (FAS form, then "
-                               "linearised) / FP64 + Anderson(3)",
+                       "path": FAST_PATH, "seeds": timed_seeds,
                        "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas x{world}"},
-            **{k: v for k, v in arm(value, info_fast).items() if k not in ("value", "unit")},
-            "learned_guess": (arm(guess_val, info_guess) if guess_val is not None else
+            **{k: v for k, v in fast_arm.items() if k not in ("value", "unit")},
+            "learned_guess": (arm(*arms["learned_guess"], "learned_guess") if "learned_guess" in arms else
                               {"unavailable": "no trained model" if guess_model is None else "skipped"}),
-            "plain_fp64_fas": arm(plain_val, info_plain) if plain_val is not None else None,
+            "fp64_fast_smoother": (arm(*arms["fp64_fast_smoother"], "fp64_fast_smoother")
+                                   if "fp64_fast_smoother" in arms else None),
+            "plain_fp64_fas": arm(*arms["plain_fp64_fas"], "plain_fp64_fas") if "plain_fp64_fas" in arms else None,
             "warm_start": warm,
             "error_vs_fp64": err,
-            "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "step_ms": ms_e2e, "timing": "each e2e step timed right after the value step of the same "
+                                                "geometry (alternating), same clock sampler"},
             "gpu_launches": fast_launches,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),
+            "summary": summary,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def oracle_check(cases, sols, workers=None):
+    """|r| / |r0| of every arm's answers, evaluated by the FP64 oracle on the
+    host cores (the checker; after the timed regions)."""
+    from oracle.check import relative_residuals
+    names = [k for k, v in sols.items() if v]
+    jobs = []
+    for k, c in enumerate(cases):
+        geo = dict(bed=c.bed, B=c.B, beta=c.beta, H_prev=c.thickness, smb=c.smb, dx=c.dx, dt=DT, thklim=c.thklim)
+        states = []
+        for name in names:
+            U = sols[name][k].numpy()
+            nu, nv = c.ny * (c.nx + 1), (c.ny + 1) * c.nx
+            states.append((U[:nu].reshape(c.ny, c.nx + 1), U[nu:nu + nv].reshape(c.ny + 1, c.nx),
+                           U[nu + nv:].reshape(c.ny, c.nx)))
+        jobs.append((geo, states))
+    rels = relative_residuals(jobs, workers=workers)
+    return {name: [r[j] for r in rels] for j, name in enumerate(names)}
 
 
 # Per-cell figures of the fine-level Vanka cell kernel with 2 local Newton
@@ -627,10 +749,11 @@ def cpu_baseline(case, infos, workers=None):
     per_step = vpc * sweeps_per_vcycle() + fin
     t_step = per_step * t_sweep
     t1 = single_thread_sweep_time(case)
-    return {"value": 1.0 / t_step, "unit": "steps/s", "cores": workers, "kind": "port",
+    return {"value": 1.0 / t_step, "unit": "steps/s", "cores": workers, "kind": "port", "modelled": True,
             "sample": f"one full-size {case.ny}x{case.nx} FP64 NumPy Vanka sweep ({t_sweep:.2f} s on {workers} "
                       f"processes), scaled by {vpc:.1f} V-cycles x {sweeps_per_vcycle():.1f} fine-equivalent "
-                      f"sweeps + {fin:.0f} finishing sweeps per step (the plain FP64 arm's counts)",
+                      f"sweeps + {fin:.0f} finishing sweeps per step (the plain FP64 arm's counts in this run)",
+            "measured_s_per_sweep": t_sweep, "sweeps_per_step": per_step,
             "single_thread": {"value": 1.0 / (per_step * t1), "unit": "steps/s", "cores": 1,
                               "sample": f"one FP64 NumPy Vanka sweep over a 128-row strip in one process, "
                                         f"scaled to {case.ny} rows ({t1:.1f} s per sweep) and to a step as above"}}
@@ -644,31 +767,45 @@ REF_FINISH_SWEEPS_PER_STEP = 937.5
 
 
 def run_reference(args):
+    """The reference arm: the reference's algorithm (plain FAS, FP64, its
+    smoother constants) in the FP64 NumPy oracle on the host cores.  A full
+    1024^2 step takes tens of minutes on a CPU, so each timed step is a
+    bounded sample -- one full-size fine-level Vanka sweep on that step's
+    geometry -- and the steps/s is modelled from it with the plain arm's
+    sweep counts; ``ms_per_step`` is the time actually measured per step."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    case = make_cases(args.n, [0])[0]
+    seeds = rank_seeds(0, args.warmup + args.steps)
     workers = os.cpu_count() or 1
     times = []
     for k in range(args.warmup + args.steps):
+        case = make_cases(args.n, [seeds[k]])[0]
         t = cpu_sweep_time(case, workers)
         if k >= args.warmup:
             times.append(t)
     t_sweep = sum(times) / len(times)
     vpc, fin = plain_step_sweeps([])
-    t_step = (vpc * sweeps_per_vcycle() + fin) * t_sweep
+    per_step = vpc * sweeps_per_vcycle() + fin
+    t_step = per_step * t_sweep
     value = 1.0 / t_step
-    sample = (f"per step: one full-size {case.ny}x{case.nx} FP64 NumPy Vanka sweep on {workers} processes "
-              f"({t_sweep:.2f} s), scaled by {vpc:g} V-cycles x {sweeps_per_vcycle():.1f} fine-equivalent sweeps "
-              f"+ {fin:g} finishing sweeps per step")
+    sample = (f"per step: one full-size {args.n}x{args.n} FP64 NumPy Vanka sweep of that step's geometry on "
+              f"{workers} processes ({t_sweep:.2f} s mean), scaled by {vpc:g} V-cycles x {sweeps_per_vcycle():.1f} "
+              f"fine-equivalent sweeps + {fin:g} finishing sweeps per step")
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded grounded-dome geometry)",
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_sweep, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded grounded-dome geometries, fresh per step)",
             "config": {"workload": f"forward step to {TOL:g} rel. residual, {args.n}x{args.n}, dx={DX:g} m, "
-                                   f"{LEVELS} levels, dt={DT:g} a", "parallelism": "host cores"},
+                                   f"{LEVELS} levels, dt={DT:g} a, fresh geometry per step",
+                       "seeds": seeds[args.warmup:], "parallelism": "host cores"},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": workers, "kind": "port", "sample": sample},
+            "modelled": {"value_is": "modelled from the measured sample", "measured_ms_per_step": 1e3 * t_sweep,
+                         "modelled_ms_per_step": 1e3 * t_step, "fine_equivalent_sweeps_per_step": per_step,
+                         "counts_source": "mean V-cycles and finishing sweeps of the plain FP64 GPU arm on these "
+                                          "geometries (constants from its last measured run)"},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": workers, "kind": "port", "modelled": True,
+                             "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -834,9 +971,111 @@ def kernel_table(args):
           flush=True)
 
 
+def _kernel_state(n):
+    """The kernel tables' inputs: the marine case at n x n with seeded random
+    velocities (the same for both implementations)."""
+    import numpy as np
+    from glide_b200.synthetic import marine_case
+    case = marine_case(0, n=n, dx=1000.0 * 4096 / n, n_levels=7)
+    rng = np.random.default_rng(0)
+    st = dict(H=case.thickness, bed=case.bed, B=case.B, beta=case.beta, f_H=case.thickness / DT + case.smb,
+              u=rng.standard_normal((n, n + 1)) * 100.0, v=rng.standard_normal((n + 1, n)) * 100.0,
+              d=rng.standard_normal(n * (n + 1) + (n + 1) * n + n * n))
+    return case, st
+
+
+def _time_ops(ops, reset=None, reps=20):
+    import torch
+    out = {}
+    for name, fn in ops.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        if reset is not None:
+            reset()
+        out[name] = round(e0.elapsed_time(e1) * 1e3 / reps, 1)
+    return out
+
+
+def kernel_compare_reference(args):
+    """The reference's own CUDA kernels (glide/cuda/*.cu built from its sources
+    into oracle/_ref, launched the way glide/grid.py launches them: FP32,
+    16x16 blocks with stride 14, zero-fills before the atomics, the host-side
+    axpy of a Vanka sweep) timed per call on the kernel tables' state, at
+    1024^2 and 4096^2.  ``bench.py --kernels-compare`` times this package's
+    kernels on the same state; profiles/ compares the two."""
+    import torch
+    from oracle import ref_replay as R
+    res = {}
+    for n in (1024, 4096):
+        case, st = _kernel_state(n)
+        g = R.RefGrid(n, n, case.dx, dt=DT)
+        for k in ("H", "bed", "B", "beta", "f_H", "u", "v"):
+            getattr(g, k).copy_(torch.as_tensor(st[k]))
+        g.gamma.fill_(0.1)
+        g.d_U.copy_(torch.as_tensor(st["d"]))
+        g.Lambda.copy_(torch.as_tensor(st["d"]))
+        saved = g.U.clone()
+        ops = {"residual": g.compute_residual, "jvp": g.compute_jvp, "vjp": g.compute_vjp,
+               "grad_beta": g.compute_grad_beta,
+               "vanka_sweep_newton10": lambda: g.vanka_sweep(1, n_inner=10),
+               "vanka_sweep_newton2": lambda: g.vanka_sweep(1, n_inner=2)}
+        res[str(n)] = _time_ops(ops, reset=lambda: g.U.copy_(saved))
+        del g
+        torch.cuda.empty_cache()
+    print(json.dumps({"impl": "reference", "kernels_us": res, "dtype": "f32",
+                      "case": "marine (floating shelves), seeded random velocities",
+                      "launch": "reference kernels built from the reference sources (sm_100a, --use_fast_math), "
+                                "glide/grid.py's launch shape and host steps"}), flush=True)
+
+
+def kernel_compare_ours(args):
+    """This package's kernels on the state of kernel_compare_reference: FP32,
+    the same operations (residual, JVP, VJP, grad_beta, one Vanka sweep with
+    the reference's smoother constants at 10 and 2 local Newton iterations)."""
+    import ctypes as C
+    import torch
+    from glide_b200 import _native as N
+    from glide_b200.grid import Grid
+    lib = N.load()
+    res = {}
+    for n in (1024, 4096):
+        case, st = _kernel_state(n)
+        g = Grid(n, n, case.dx, dt=DT, dtype=torch.float32)
+        for k in ("H", "bed", "B", "beta", "f_H", "u", "v"):
+            getattr(g, k).copy_(torch.as_tensor(st[k]))
+        g.gamma.fill_(0.1)
+        g.d_U.copy_(torch.as_tensor(st["d"]))
+        g.Lambda.copy_(torch.as_tensor(st["d"]))
+        grad = torch.empty_like(g.H)
+        a = g.level_args()
+        s = torch.cuda.current_stream().cuda_stream
+        saved = g.U.clone()
+        ops = {"residual": g.compute_residual, "jvp": g.compute_jvp, "vjp": g.compute_vjp,
+               "grad_beta": lambda: lib.glide_grad_beta(C.byref(a), g.lambda_u.data_ptr(), g.lambda_v.data_ptr(),
+                                                        grad.data_ptr(), 0, s),
+               "vanka_sweep_newton10": lambda: g.vanka_sweep(1, n_inner=10, omega=0.5, shift=1.0, step=0.25),
+               "vanka_sweep_newton2": lambda: g.vanka_sweep(1, n_inner=2, omega=0.5, shift=1.0, step=0.25)}
+        res[str(n)] = _time_ops(ops, reset=lambda: g.U.copy_(saved))
+        del g
+        torch.cuda.empty_cache()
+    print(json.dumps({"impl": "ours", "kernels_us": res, "dtype": "f32",
+                      "case": "marine (floating shelves), seeded random velocities"}), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.impl == "reference" and args.kernels_compare:
+        kernel_compare_reference(args)
+    elif args.kernels_compare:
+        kernel_compare_ours(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.kernels:
         kernel_table(args)
