@@ -75,6 +75,8 @@ def parse():
                     help="mixed vs FP64 on the 512^2 100-step and the 4096^2 20-step configurations (one JSON line)")
     ap.add_argument("--configs-only", default=None, help="with --configs: only the configuration named so")
     ap.add_argument("--configs-steps", type=int, default=0, help="with --configs: steps per series (0: 100 / 20)")
+    ap.add_argument("--configs-iters", type=int, default=200, help="with --configs: L-BFGS iterations of the inversion")
+    ap.add_argument("--configs-fd", type=int, default=16, help="with --configs: finite-difference directions")
     return ap.parse_args()
 
 
@@ -201,6 +203,8 @@ FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step
                finish_fas_until=2e-4, finish_fas_patience=8,
                newton=True, newton_start=1e-2, newton_after=200, newton_min_gain=4.0, newton_local=2,
                newton_max_steps=6)
+# the same-branch reference solves (TOL_TIGHT): the fast path's settings with the sweeps-only finish
+TIGHT_KW = {k: v for k, v in FAST_KW.items() if not k.startswith("newton")}
 # the fast path's smoother and finishing rule in FP64 (no FP32 correction stages)
 FP64_FAST_KW = dict(finish_anderson=3, finish_newton=2, finish_step=1.0)
 FAST_PATH = ("mixed FAS, full-step local Newton x2, finishing sweeps FP32 (FAS form, then linearised) / FP64 + "
@@ -240,6 +244,23 @@ class Runner:
             guess = self.guess_model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"])
         ph.forward(DT, tol=TOL if tol is None else tol, max_vcycles=self.max_vcycles, guess=guess,
                    max_finish_sweeps=max_finish_sweeps)
+        return dict(ph.last_info)
+
+    def continue_step(self, dev, U, tol, max_finish_sweeps=MAX_FINISH):
+        """Continue a solved step of the geometry ``dev`` from the state ``U``
+        (a host or device FP64 vector) to ``tol``, relative to the residual of
+        the step's starting state (so the answer stays on U's solution branch)."""
+        ph = self.ph
+        ph.set_geometry(dev["bed"], dev["H"])
+        ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
+        ph.reset_solution()
+        ph._set_dt(DT)
+        g = ph.grid
+        g.f_H.copy_(g.H_prev / DT + g.smb)
+        r0 = ph.residual_norm()
+        g.U.copy_(U.to(device=g.U.device, dtype=g.U.dtype))
+        ph.forward(DT, tol=tol, max_vcycles=self.max_vcycles, max_finish_sweeps=max_finish_sweeps, r0=r0,
+                   update_geometry=False)
         return dict(ph.last_info)
 
 
@@ -553,11 +574,18 @@ def run_ours(args):
 
     # accuracy of the fast path's answers: against the same solve continued to
     # TOL_TIGHT (its residual is evaluated in FP64, so that state solves the
-    # FP64 discrete equations to TOL_TIGHT, on the same solution branch)
+    # FP64 discrete equations to TOL_TIGHT, on the same solution branch); it
+    # continues from each fast answer with the finishing sweeps alone (the
+    # Newton-Krylov finish is tuned for TOL and can stall short of TOL_TIGHT
+    # at the non-smooth cells of the mass balance)
+    tight = Runner(n, "mixed", None, args.max_vcycles, fast_settings(), use_graphs=not args.eager, **TIGHT_KW)
     sol_tight, rel_tight = [], []
     for k in range(args.steps):
-        rel_tight.append(fast.step(fdev[args.warmup + k], tol=TOL_TIGHT)["rel_residual"])
-        sol_tight.append(fast.ph.grid.U.detach().to(torch.float64).cpu())
+        info = tight.continue_step(fdev[args.warmup + k], sols["fast"][k], TOL_TIGHT)
+        rel_tight.append(info["rel_residual"])
+        sol_tight.append(tight.ph.grid.U.detach().to(torch.float64).cpu())
+    del tight
+    torch.cuda.empty_cache()
     kept = [k for k, r in enumerate(rel_tight) if r is not None and r <= TOL_TIGHT]
     err = {"fast": solution_error([sols["fast"][k] for k in kept], [sol_tight[k] for k in kept], n) if kept else None,
            "reference_solution": f"the same solve continued to {TOL_TIGHT:g} relative residual (FP64 residual)",
@@ -857,6 +885,74 @@ def config_series(case, precision, steps, cot_seed=7):
     return state, grad, t, rels, adj_rel
 
 
+def config_inversion(args, n=512, steps=50, every=10, iters=200, fd_dirs=16, eps=1e-6, seed=0):
+    """Inversion of log beta on the plain-method dome at n x n (same domain:
+    dx = 5 km * 64 / n): observations from a true log beta = log(1e3 Pa a/m)
+    + a Gaussian random field (20 km correlation, sigma 1) after ``steps``
+    implicit steps, with 2 % proportional Gaussian noise; the model runs the
+    same steps checkpointed every ``every`` with recomputation (the
+    hand-written VJP behind torch.autograd); central differences on
+    ``fd_dirs`` seeded directions (eps = 1e-6, FP64, steps solved to 1e-10);
+    L-BFGS-B for ``iters`` iterations (mixed precision, steps and adjoints
+    to TOL) with Tikhonov weight 1e-3 on log beta."""
+    import numpy as np
+    import torch
+    from glide_b200 import IcePhysics
+    from glide_b200.adjoint import time_stepped
+    from glide_b200.inverse import TimeSteppedObjective, finite_difference_check, invert_time_stepped
+    from glide_b200.synthetic import _grf, beta_head, dome_case
+    steps = args.configs_steps or steps
+    c = dome_case(seed, n=n, dx=5000.0 * 64 / n, n_levels=5)
+    rng = np.random.default_rng(seed + 1)
+    logb_ref = float(np.log(beta_head(1e3)))
+    logb_true = logb_ref + _grf(rng, n, n, c.dx, 20e3)
+
+    def physics(precision):
+        kw = dict(settings=fast_settings(), **(FAST_KW if precision == "mixed" else FP64_FAST_KW))
+        ph = IcePhysics(n, n, c.dx, n_levels=c.n_levels, thklim=c.thklim, precision=precision, **kw)
+        ph.set_geometry(c.bed, c.thickness)
+        ph.set_parameters(B=c.B, beta=np.exp(logb_true), smb=c.smb)
+        return ph
+
+    ph = physics("mixed")
+    H0 = torch.as_tensor(c.thickness, device="cuda")
+    t0 = time.time()
+    with torch.no_grad():
+        u, v, _ = time_stepped(torch.exp(torch.as_tensor(logb_true, device="cuda")), H0, ph, c.dt, steps, every,
+                               1e-8, 1e-8, 60)
+        u_obs = u * (1.0 + 0.02 * torch.randn(u.shape, generator=torch.Generator().manual_seed(5),
+                                              dtype=u.dtype).to(u.device))
+        v_obs = v * (1.0 + 0.02 * torch.randn(v.shape, generator=torch.Generator().manual_seed(6),
+                                              dtype=v.dtype).to(v.device))
+    t_obs = time.time() - t0
+    x0 = np.full(n * n, logb_ref)
+    out = {"grid": f"{n}x{n}, dx={c.dx:g} m, {c.n_levels} levels, dt={c.dt:g} a", "steps": steps,
+           "checkpoint_every": every, "observations_s": t_obs}
+    # gradient check in FP64
+    ph64 = physics("fp64")
+    obj64 = TimeSteppedObjective(ph64, H0, u_obs, v_obs, c.dt, steps, every, reg_weight=1e-3, tol=1e-10,
+                                 adj_tol=1e-10)
+    t0 = time.time()
+    errs, pairs = finite_difference_check(obj64, x0, n_directions=fd_dirs, eps=eps)
+    out["fd_check"] = {"directions": fd_dirs, "eps": eps, "rel_err": errs, "max_rel_err": max(errs),
+                       "median_rel_err": float(np.median(errs)), "s": time.time() - t0,
+                       "max_step_rel_residual": obj64.max_step_rel, "tol": 1e-10}
+    del obj64, ph64
+    torch.cuda.empty_cache()
+    # L-BFGS in mixed precision
+    obj = TimeSteppedObjective(ph, H0, u_obs, v_obs, c.dt, steps, every, reg_weight=1e-3, tol=TOL, adj_tol=TOL)
+    t0 = time.time()
+    x, rec = invert_time_stepped(obj, x0, maxiter=iters)
+    t_inv = time.time() - t0
+    err0 = float(np.sqrt(np.mean((x0 - logb_true.ravel()) ** 2)))
+    err1 = float(np.sqrt(np.mean((x - logb_true.ravel()) ** 2)))
+    out["lbfgs"] = {**rec, "s": t_inv, "s_per_evaluation": t_inv / max(rec["evaluations"] - 1, 1),
+                    "tol": TOL, "max_step_rel_residual": obj.max_step_rel,
+                    "misfit_reduction": rec["final"]["misfit"] / rec["initial"]["misfit"],
+                    "log_beta_rms_error": {"start": err0, "final": err1}}
+    return out
+
+
 def run_configs(args):
     """The 512^2 continental time series and the 4096^2 marine case, the
     fast mixed-precision path against plain FP64, every step and the final
@@ -870,6 +966,8 @@ def run_configs(args):
     out = {}
     specs = [("c2_continental_512", ice_sheet_case(0, n=512, dx=1500.0, n_levels=5), args.configs_steps or 100),
              ("c5_marine_4096", marine_case(0, n=4096, dx=1000.0, n_levels=7), args.configs_steps or 20)]
+    if not args.configs_only or "c3" in args.configs_only:
+        out["c3_inversion_512"] = config_inversion(args, iters=args.configs_iters, fd_dirs=args.configs_fd)
     for name, case, steps in specs:
         if args.configs_only and args.configs_only not in name:
             continue

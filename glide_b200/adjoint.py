@@ -15,8 +15,9 @@ held at the thickness limit (mask m: H <= gamma + 0.1, glide/grid.py:332)
 are identity rows of J, so they pass no sensitivity to H_prev.
 
 ``TimeStepper`` chains n steps; its backward recomputes each segment of
-``checkpoint_every`` steps from a stored thickness (the only state carried
-between steps) before running the adjoint steps of that segment in reverse.
+``checkpoint_every`` steps once from a stored thickness (the only state
+carried between steps), keeps the segment's solved states, and runs the
+adjoint steps of that segment in reverse at those states.
 """
 from __future__ import annotations
 
@@ -32,8 +33,36 @@ def _solve(physics, beta, H_prev, dt, tol, max_vcycles):
         physics.grid32.H_prev.copy_(H_prev)
     g.u.zero_()
     g.v.zero_()
-    physics.forward(dt, tol=tol, max_vcycles=max_vcycles, update_geometry=False)
+    physics.forward(dt, tol=tol, max_vcycles=max_vcycles, update_geometry=False, max_finish_sweeps=20000)
+    log = getattr(physics, "solve_log", None)
+    if isinstance(log, list):   # relative residual each solve reached (diagnostics of callers)
+        log.append(physics.last_info.get("rel_residual"))
     return g.u.clone(), g.v.clone(), g.H.clone()
+
+
+def _restore(physics, beta, H_prev, U, dt):
+    """Put a solved step back as the linearisation point of its adjoint
+    (parameters, H_prev, dt and the converged state) without solving again.
+    The coarse levels, where the adjoint V-cycle linearises its coarse
+    corrections, get the restricted state, so the adjoint depends on the
+    step's state alone (not on which solve ran last)."""
+    from .kernels import restrict_cell_centered, restrict_hfacet, restrict_vfacet
+    g = physics.grid
+    physics.set_parameters(beta=beta)
+    physics._set_dt(dt)
+    g.H_prev.copy_(H_prev)
+    if physics.grid32 is not None:
+        physics.grid32.H_prev.copy_(H_prev)
+        physics.grid32.U.copy_(U)
+        hier = physics.grids32
+    else:
+        hier = physics.grids
+    g.U.copy_(U)
+    g.f_H.copy_(g.H_prev / dt + g.smb)
+    for par, ch in zip(hier[:-1], hier[1:]):
+        restrict_vfacet(par.u, u_coarse=ch.u)
+        restrict_hfacet(par.v, v_coarse=ch.v)
+        restrict_cell_centered(par.H, f_coarse=ch.H)
 
 
 def _adjoint(physics, du, dv, dH, dt, adj_tol, max_vcycles):
@@ -105,14 +134,17 @@ class TimeStepper(torch.autograd.Function):
         starts = sorted(ctx.checkpoints)
         for s0 in reversed(starts):
             s1 = min(s0 + every, n)
-            # recompute the segment, keeping each step's starting thickness
-            Hs = [ctx.checkpoints[s0]]
-            for k in range(s0, s1 - 1):
-                _, _, Hn = _solve(ph, beta, Hs[-1], dt, ctx.tol, ctx.max_vcycles)
-                Hs.append(Hn)
-            for k in range(s1 - 1, s0 - 1, -1):
-                H_in = Hs[k - s0]
+            # recompute the segment once, keeping each step's starting thickness and solved state
+            steps = []
+            H_in = ctx.checkpoints[s0]
+            for k in range(s0, s1):
                 u, v, H = _solve(ph, beta, H_in, dt, ctx.tol, ctx.max_vcycles)
+                steps.append((H_in, ph.grid.U.detach().clone()))
+                H_in = H
+            for k in range(s1 - 1, s0 - 1, -1):
+                H_in, U = steps[k - s0]
+                _restore(ph, beta, H_in, U, dt)
+                u, v, H = ph.grid.u, ph.grid.v, ph.grid.H
                 z = lambda t, like: torch.zeros_like(like) if t is None else t
                 gb, gh = _adjoint(ph, z(cu, u), z(cv, v), z(cH, H), dt, ctx.adj_tol, ctx.max_vcycles)
                 grad_beta += gb.to(grad_beta.dtype)

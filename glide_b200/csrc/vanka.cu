@@ -479,7 +479,10 @@ template <typename T, bool LOCAL>
 #ifndef GLIDE_VANKA64_MIN_BLOCKS
 #define GLIDE_VANKA64_MIN_BLOCKS 2
 #endif
-__global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? 2 : GLIDE_VANKA64_MIN_BLOCKS) vanka_cells_kernel(
+#ifndef GLIDE_VANKA32_MIN_BLOCKS
+#define GLIDE_VANKA32_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(VNT, sizeof(T) == 4 ? GLIDE_VANKA32_MIN_BLOCKS : GLIDE_VANKA64_MIN_BLOCKS) vanka_cells_kernel(
     T* __restrict__ scratch, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ H,
     const T* __restrict__ f_u, const T* __restrict__ f_v, const T* __restrict__ f_H, const T* __restrict__ bed,
     const T* __restrict__ B, const T* __restrict__ beta, const T* __restrict__ gamma, const int* __restrict__ flags,

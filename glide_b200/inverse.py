@@ -164,3 +164,108 @@ def invert_beta(physics, u_obs, v_obs, dt, *, reg_weight=1e-4, loss="abs", bound
         if pos + 1 < len(order) and order[pos + 1] == k - 1:
             prolongate_cell_centered(g.beta, H_fine=grids[k - 1].beta)
     return physics.grid.beta, records
+
+
+# ---------------------------------------------------------------------------
+# time-stepped inversion (no counterpart in the reference, whose adjoint is
+# single-step, glide/physics.py:211-242)
+# ---------------------------------------------------------------------------
+class TimeSteppedObjective:
+    """L(log beta) = 1/2 |u_n - u_obs|^2 + 1/2 |v_n - v_obs|^2 + reg_weight * T(log beta)
+    after ``n_steps`` implicit steps from H0, and its gradient in log beta.
+
+    The steps run through ``glide_b200.adjoint.TimeStepper`` (checkpoints every
+    ``checkpoint_every`` steps, segments recomputed in the backward pass); the
+    misfit gradient is beta * dL/dbeta from the hand-written adjoint, the
+    Tikhonov term (``losses.tikhonov``) is taken in log beta directly.
+    ``x`` is the flattened log beta (float64 NumPy), as scipy's L-BFGS-B
+    passes it."""
+
+    def __init__(self, physics, H0, u_obs, v_obs, dt, n_steps, checkpoint_every=10, reg_weight=1e-3, tol=1e-8,
+                 adj_tol=1e-8, max_vcycles=60):
+        g = physics.grid
+        self.ph, self.dt, self.n, self.every = physics, float(dt), int(n_steps), int(checkpoint_every)
+        self.H0 = torch.as_tensor(H0, dtype=g.dtype, device=g.device)
+        self.u_obs = torch.as_tensor(u_obs, dtype=g.dtype, device=g.device)
+        self.v_obs = torch.as_tensor(v_obs, dtype=g.dtype, device=g.device)
+        self.reg_weight, self.tol, self.adj_tol, self.max_vcycles = float(reg_weight), tol, adj_tol, max_vcycles
+        self.shape = (g.ny, g.nx)
+        self.evaluations = 0
+        self.max_step_rel = 0.0   # largest |r|/|r0| any step of any evaluation reached
+        self.last = {}
+
+    def value_and_grad(self, logb):
+        """Objective and gradient for a log-beta tensor (device, working dtype)."""
+        from .adjoint import time_stepped
+        beta = torch.exp(logb.detach()).requires_grad_(True)
+        self.ph.solve_log = []
+        u, v, _ = time_stepped(beta, self.H0, self.ph, self.dt, self.n, self.every, self.tol, self.adj_tol,
+                               self.max_vcycles)
+        J = 0.5 * ((u - self.u_obs) ** 2).sum() + 0.5 * ((v - self.v_obs) ** 2).sum()
+        J.backward()
+        t, gt = tikhonov(logb.detach())
+        grad = beta.grad * beta.detach() + self.reg_weight * gt
+        total = float(J.detach()) + self.reg_weight * float(t)
+        self.evaluations += 1
+        rels = [r for r in self.ph.solve_log if r is not None]
+        self.ph.solve_log = None
+        self.last = {"misfit": float(J.detach()), "reg": self.reg_weight * float(t), "total": total,
+                     "max_step_rel_residual": max(rels) if rels else None,
+                     "adjoint_rel_residual": getattr(self.ph, "last_adjoint_info", {}).get("rel_residual")}
+        self.max_step_rel = max(self.max_step_rel, max(rels) if rels else 0.0)
+        return total, grad
+
+    def _logb(self, x):
+        g = self.ph.grid
+        return torch.as_tensor(np.asarray(x).reshape(self.shape), dtype=g.dtype, device=g.device)
+
+    def __call__(self, x):
+        total, grad = self.value_and_grad(self._logb(x))
+        return total, grad.double().cpu().numpy().ravel()
+
+    def value(self, x):
+        """The objective alone (forward steps only, no adjoint)."""
+        from .adjoint import time_stepped
+        logb = self._logb(x)
+        self.ph.solve_log = []
+        with torch.no_grad():
+            u, v, _ = time_stepped(torch.exp(logb), self.H0, self.ph, self.dt, self.n, self.every, self.tol,
+                                   self.adj_tol, self.max_vcycles)
+            J = 0.5 * ((u - self.u_obs) ** 2).sum() + 0.5 * ((v - self.v_obs) ** 2).sum()
+        rels = [r for r in self.ph.solve_log if r is not None]
+        self.ph.solve_log = None
+        self.max_step_rel = max(self.max_step_rel, max(rels) if rels else 0.0)
+        t, _ = tikhonov(logb)
+        return float(J) + self.reg_weight * float(t)
+
+
+def finite_difference_check(objective, x, n_directions=16, eps=1e-6, seed=0):
+    """Central differences (L(x + eps d) - L(x - eps d)) / (2 eps) of a
+    ``TimeSteppedObjective`` along ``n_directions`` seeded unit-variance
+    directions d, against grad . d from its adjoint.  Returns the relative
+    differences |fd - ad| / |fd| and the pairs (fd, ad)."""
+    rng = np.random.default_rng(seed)
+    _, grad = objective(x)
+    errs, pairs = [], []
+    for _ in range(n_directions):
+        d = rng.standard_normal(x.size)
+        fp = objective.value(x + eps * d)
+        fm = objective.value(x - eps * d)
+        fd = (fp - fm) / (2.0 * eps)
+        ad = float(grad @ d)
+        errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+        pairs.append((fd, ad))
+    return errs, pairs
+
+
+def invert_time_stepped(objective, x0, *, maxiter=200, bounds=(-6.0, 5.0), m=15, factr=1e7, callback=None):
+    """L-BFGS-B over log beta of a ``TimeSteppedObjective`` (``maxiter``
+    iterations at most).  Returns the optimum and a record."""
+    from scipy.optimize import fmin_l_bfgs_b
+    f0, _ = objective(x0)
+    first = dict(objective.last)
+    x, f, info = fmin_l_bfgs_b(objective, x0, bounds=[bounds] * x0.size, m=m, factr=factr, maxiter=maxiter,
+                               callback=callback)
+    return x, {"initial": first, "final": dict(objective.last), "final_total": float(f),
+               "iterations": int(info["nit"]), "evaluations": objective.evaluations,
+               "warnflag": int(info["warnflag"])}

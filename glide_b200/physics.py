@@ -346,12 +346,15 @@ class IcePhysics:
 
     # ------------------------------------------------------------------ API
     def forward(self, dt, n_vcycles=3, verbose=False, update_geometry=True, *, tol=None, max_vcycles=100,
-                guess=None, history=None, finish=True, max_finish_sweeps=4000):
+                guess=None, history=None, finish=True, max_finish_sweeps=4000, r0=None):
         """One implicit time step (glide/physics.py:141-209).
 
         Without ``tol`` runs ``n_vcycles`` cycles like the reference.  With
         ``tol`` runs cycles until |r|/|r0| <= tol; with ``finish`` a stalled
         cycle hands over to FP64 fine-level relaxation (see the module doc).
+        ``r0`` (with ``tol``) continues an earlier solve of the same step from
+        the current state: |r0| is then the given norm of the step's starting
+        residual instead of the residual of the current state.
         ``last_info`` records cycles, finishing sweeps, the residual reached
         and whether a guess was used or dropped.
         """
@@ -361,7 +364,8 @@ class IcePhysics:
         if self.grid32 is not None:
             self.grid32.f_H.copy_(g.f_H)  # overwritten by the correction RHS, kept for API reads
         track = tol is not None or verbose or history is not None or guess is not None
-        r0 = self.residual_norm() if track else None
+        if r0 is None or tol is None:
+            r0 = self.residual_norm() if track else None
         hist = [1.0] if track else []
         info = {"vcycles": 0, "finish_sweeps": 0, "guess_used": False, "fallback": False}
         if verbose:

@@ -4,7 +4,9 @@ The reference kernels are built from the reference tree into
 ``oracle/_ref/libglide_ref.so`` (``oracle/build_ref.py``) and travel with the
 repository snapshot; the test is skipped when that library is absent.
 Tolerances (norm-wise relative error, FP32 vs FP32 fast-math):
-  single operators <= 2e-5; one Vanka sweep <= 1e-4; one forward step <= 5e-3.
+  single operators <= 2e-5; one Vanka sweep <= 1e-4; one forward step
+  (1 V-cycle, reference settings, 64^2 dome) <= 1e-6 -- measured 1.8e-7 (u),
+  1.7e-7 (v), 3.3e-8 (H) on a B200.
 """
 import numpy as np
 import pytest
@@ -99,5 +101,7 @@ def test_forward_step_vs_reference():
         ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
     a = mine.forward(c.dt, n_vcycles=1)
     b = ref.forward(c.dt, n_vcycles=1)
-    for x, y in zip(a, b):
-        assert rel(x, y) <= 5e-3
+    errs = [rel(x, y) for x, y in zip(a, b)]
+    print("forward step vs reference kernels (u, v, H):", errs)
+    for e in errs:
+        assert e <= 1e-6
