@@ -205,8 +205,10 @@ FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step
                newton_max_steps=6)
 # the same-branch reference solves (TOL_TIGHT): the fast path's settings with the sweeps-only finish
 TIGHT_KW = {k: v for k, v in FAST_KW.items() if not k.startswith("newton")}
-# the fast path's smoother and finishing rule in FP64 (no FP32 correction stages)
-FP64_FAST_KW = dict(finish_anderson=3, finish_newton=2, finish_step=1.0)
+# the fast path's smoother and finishing rule in FP64 (no FP32 correction stages; the
+# Newton-Krylov finish on the FP64 hierarchy)
+FP64_FAST_KW = dict(finish_anderson=3, finish_newton=2, finish_step=1.0,
+                    **{k: v for k, v in FAST_KW.items() if k.startswith("newton")})
 FAST_PATH = ("mixed FAS, full-step local Newton x2, finishing sweeps FP32 (FAS form, then linearised) / FP64 + "
              "Anderson(3); after 200 sweeps a Newton-Krylov finish (FGMRES, linear multigrid V-cycle "
              "preconditioner) while its steps gain >= 4x")
@@ -838,19 +840,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def config_series(case, precision, steps, cot_seed=7):
+def config_series(case, precision, steps, cot_seed=7, arm="fast", newton=None):
     """``steps`` implicit steps of one geometry, each started from the
-    previous one and solved to |r|/|r0| <= TOL (mixed: the fast path; FP64:
-    the plain FAS arm's settings), then the adjoint gradient of a seeded
-    cotangent of (u, v) through the last step, solved to the same relative
-    tolerance.  Returns the final state, the gradient, the time of the steps
-    and the relative residual each step reached."""
+    previous one and solved to |r|/|r0| <= TOL, then the adjoint gradient of
+    a seeded cotangent of (u, v) through the last step, solved to the same
+    relative tolerance.  ``arm`` "fast": the fast path's solver (mixed, or
+    the same solver in FP64); "plain": the plain FAS arm's settings.
+    ``newton`` overrides the Newton-Krylov options.  Returns the final state,
+    the gradient, the time of the steps and the relative residual each step
+    reached."""
     import torch
     from glide_b200 import IcePhysics
-    if precision == "mixed":
-        kw = dict(settings=fast_settings(), **FAST_KW)
-    else:
+    if arm == "plain":
         kw = dict(settings=tol_settings())
+    else:
+        kw = dict(settings=fast_settings(), **(FAST_KW if precision == "mixed" else FP64_FAST_KW))
+        kw.update(newton or {})
     ph = IcePhysics(case.ny, case.nx, case.dx, n_levels=case.n_levels, thklim=case.thklim, precision=precision,
                     **kw, **case.kwargs)
 
@@ -867,7 +872,7 @@ def config_series(case, precision, steps, cot_seed=7):
     rels = []
     a.record()
     for _ in range(steps):
-        ph.forward(case.dt, tol=TOL, max_vcycles=40)
+        ph.forward(case.dt, tol=TOL, max_vcycles=40, max_finish_sweeps=MAX_FINISH)
         rels.append(ph.last_info["rel_residual"])
     b.record()
     torch.cuda.synchronize()
@@ -878,7 +883,8 @@ def config_series(case, precision, steps, cot_seed=7):
     cu = torch.randn(tuple(g.u.shape), generator=gen, dtype=torch.float64).to(g.u.device, g.dtype)
     cv = torch.randn(tuple(g.v.shape), generator=gen, dtype=torch.float64).to(g.u.device, g.dtype)
     # the adjoint linearises at the last step's state
-    grad = ph.adjoint(cu, cv, torch.zeros_like(g.H), tol=TOL, max_vcycles=40).detach().to(torch.float64).clone()
+    grad = ph.adjoint(cu, cv, torch.zeros_like(g.H), tol=TOL, max_vcycles=40,
+                      max_finish_sweeps=MAX_FINISH).detach().to(torch.float64).clone()
     adj_rel = ph.last_adjoint_info.get("rel_residual")
     del ph
     torch.cuda.empty_cache()
@@ -908,7 +914,10 @@ def config_inversion(args, n=512, steps=50, every=10, iters=200, fd_dirs=16, eps
     logb_true = logb_ref + _grf(rng, n, n, c.dx, 20e3)
 
     def physics(precision):
-        kw = dict(settings=fast_settings(), **(FAST_KW if precision == "mixed" else FP64_FAST_KW))
+        # the FP64 model of the finite differences is solved to 1e-10: sweeps-only finish
+        kw = dict(settings=fast_settings(),
+                  **(FAST_KW if precision == "mixed" else {k: v for k, v in FP64_FAST_KW.items()
+                                                           if not k.startswith("newton")}))
         ph = IcePhysics(n, n, c.dx, n_levels=c.n_levels, thklim=c.thklim, precision=precision, **kw)
         ph.set_geometry(c.bed, c.thickness)
         ph.set_parameters(B=c.B, beta=np.exp(logb_true), smb=c.smb)
@@ -964,20 +973,24 @@ def run_configs(args):
         return float((a - b).norm() / b.norm().clamp_min(1e-300))
 
     out = {}
-    specs = [("c2_continental_512", ice_sheet_case(0, n=512, dx=1500.0, n_levels=5), args.configs_steps or 100),
-             ("c5_marine_4096", marine_case(0, n=4096, dx=1000.0, n_levels=7), args.configs_steps or 20)]
+    # at 4096^2 the finishing sweeps converge too slowly to wait for: Newton-Krylov as soon as |r|/|r0| <= 1e-2
+    nk_4096 = dict(newton_after=0, newton_min_gain=1.0, newton_max_steps=12)
+    specs = [("c2_continental_512", ice_sheet_case(0, n=512, dx=1500.0, n_levels=5), args.configs_steps or 100, None),
+             ("c5_marine_4096", marine_case(0, n=4096, dx=1000.0, n_levels=7), args.configs_steps or 20, nk_4096)]
     if not args.configs_only or "c3" in args.configs_only:
         out["c3_inversion_512"] = config_inversion(args, iters=args.configs_iters, fd_dirs=args.configs_fd)
-    for name, case, steps in specs:
+    for name, case, steps, nk in specs:
         if args.configs_only and args.configs_only not in name:
             continue
         res = {}
         for prec in ("mixed", "fp64"):
-            res[prec] = config_series(case, prec, steps)
+            res[prec] = config_series(case, prec, steps, newton=nk)
         (sm, gm, tm, rm, am), (sd, gd, td, rd, ad) = res["mixed"], res["fp64"]
         out[name] = {
             "grid": f"{case.ny}x{case.nx}, dx={case.dx:g} m, {case.n_levels} levels, dt={case.dt:g} a",
             "steps": steps, "tol": TOL, "series": "each step started from the previous one",
+            "fp64_arm": "the same solver in FP64 (fast smoother, Newton-Krylov on the FP64 hierarchy)",
+            "newton": nk or {k: v for k, v in FAST_KW.items() if k.startswith("newton")},
             "mixed_steps_per_s": steps / tm, "fp64_steps_per_s": steps / td, "speedup": td / tm,
             "max_rel_residual": {"mixed": max(rm), "fp64": max(rd)},
             "adjoint_rel_residual": {"mixed": am, "fp64": ad},

@@ -125,8 +125,8 @@ def load():
         "glide_linear_setup": [C.POINTER(Level), i, C.POINTER(SolverConfig), vp],
         "glide_linear_vcycle": [C.POINTER(Level), i, C.POINTER(SolverConfig), vp],
         "glide_vanka_lu_masked": [LA, vp, d, vp],
-        "glide_newton_rhs": [LA, vp, vp, vp, vp, vp],
-        "glide_newton_update": [LA, vp, vp, vp, d, vp],
+        "glide_newton_rhs": [LA, vp, vp, vp, vp, i, vp],
+        "glide_newton_update": [LA, vp, vp, vp, i, d, vp],
         "glide_active_mask": [LA, vp, vp, vp],
         "glide_dots": [i, i64, i, vp, i64, vp, vp, vp, vp],
         "glide_dots_parts": [i64],

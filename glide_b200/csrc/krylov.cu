@@ -84,26 +84,28 @@ __global__ void __launch_bounds__(KB) combine_k(T* __restrict__ out, const T* __
     }
 }
 
-// Right-hand side of one Newton step in mixed precision.  r is the FP64
-// residual F(U) - f of the state (faces first, then cells); a cell is in the
-// active set when H - dt r_H <= gamma (the Vanka smoother's rule), and its row
-// becomes the constraint H - gamma.  rhs32 = fl32(masked r), rraw32 =
-// fl32(r), mask32 = the active set.
-__global__ void newton_rhs_k(float* __restrict__ rhs32, float* __restrict__ rraw32, float* __restrict__ mask32,
+// Right-hand side of one Newton step.  r is the FP64 residual F(U) - f of
+// the state (faces first, then cells); a cell is in the active set when
+// H - dt r_H <= gamma (the Vanka smoother's rule), and its row becomes the
+// constraint H - gamma.  rhs = masked r, rraw = r and mask = the active set,
+// all in the linear solver's precision TO (FP32 for the mixed path, FP64 for
+// the FP64 path).
+template <typename TO>
+__global__ void newton_rhs_k(TO* __restrict__ rhs, TO* __restrict__ rraw, TO* __restrict__ mask,
                              const double* __restrict__ r, const double* __restrict__ H,
                              const double* __restrict__ gamma, double dt, int64_t n_faces, int64_t n_cells) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k < n_faces) {
-        const float x = float(r[k]);
-        rhs32[k] = x;
-        rraw32[k] = x;
+        const TO x = TO(r[k]);
+        rhs[k] = x;
+        rraw[k] = x;
     } else if (k < n_faces + n_cells) {
         const int64_t c = k - n_faces;
         const double rH = r[k];
         const bool act = H[c] - dt * rH <= gamma[c];
-        mask32[c] = act ? 1.0f : 0.0f;
-        rhs32[k] = float(act ? H[c] - gamma[c] : rH);
-        rraw32[k] = float(rH);
+        mask[c] = act ? TO(1) : TO(0);
+        rhs[k] = TO(act ? H[c] - gamma[c] : rH);
+        rraw[k] = TO(rH);
     }
 }
 
@@ -115,8 +117,10 @@ __global__ void active_mask_k(T* __restrict__ mask, const T* __restrict__ H, con
     if (k < n) mask[k] = H[k] - dt * r_H[k] <= gamma[k] ? T(1) : T(0);
 }
 
-// U = base + alpha * fl64(d) with H kept >= gamma (FP64 state, FP32 correction).
-__global__ void newton_update_k(double* __restrict__ U, const double* __restrict__ base, const float* __restrict__ d,
+// U = base + alpha * d with H kept >= gamma (FP64 state; d in the linear
+// solver's precision TD).
+template <typename TD>
+__global__ void newton_update_k(double* __restrict__ U, const double* __restrict__ base, const TD* __restrict__ d,
                                 double alpha, const double* __restrict__ gamma, int64_t n_faces, int64_t n_cells) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= n_faces + n_cells) return;
@@ -127,16 +131,21 @@ __global__ void newton_update_k(double* __restrict__ U, const double* __restrict
 
 static inline unsigned nblocks(int64_t n) { return unsigned((n + KB - 1) / KB); }
 
+// At most 16 vectors per pass (16 FP64 accumulators keep the kernel near 80
+// registers and the SM full of warps); more vectors take a second pass.
 template <typename T>
 int launch_dots(int64_t n, int k, const void* V, int64_t ldv, const void* w, double* out, double* parts,
                 cudaStream_t s) {
     const int nb = dots_parts_count(n);
-    if (k <= 8)
-        glide::count_launch(), multidot_partial_k<T, 8><<<nb, KB, 0, s>>>(parts, (const T*)V, ldv, (const T*)w, n, k);
-    else
-        glide::count_launch(), multidot_partial_k<T, DOT_KMAX><<<nb, KB, 0, s>>>(parts, (const T*)V, ldv,
-                                                                                 (const T*)w, n, k);
-    glide::count_launch(), multidot_final_k<<<k, KB, 0, s>>>(out, parts, nb, k);
+    for (int i0 = 0; i0 < k; i0 += 16) {
+        const int kk = k - i0 < 16 ? k - i0 : 16;
+        const T* Vi = (const T*)V + int64_t(i0) * ldv;
+        if (kk <= 8)
+            glide::count_launch(), multidot_partial_k<T, 8><<<nb, KB, 0, s>>>(parts, Vi, ldv, (const T*)w, n, kk);
+        else
+            glide::count_launch(), multidot_partial_k<T, 16><<<nb, KB, 0, s>>>(parts, Vi, ldv, (const T*)w, n, kk);
+        glide::count_launch(), multidot_final_k<<<kk, KB, 0, s>>>(out + i0, parts, nb, kk);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -175,16 +184,21 @@ int glide_combine(int dtype, int64_t n, int k, const void* V, int64_t ldv, const
                               : launch_combine<double>(n, k, V, ldv, coef, alpha, out, beta, (cudaStream_t)stream);
 }
 
-int glide_newton_rhs(const GlideLevelArgs* a64, const void* r64, void* rhs32, void* rraw32, void* mask32,
+int glide_newton_rhs(const GlideLevelArgs* a64, const void* r64, void* rhs, void* rraw, void* mask, int lin_dtype,
                      void* stream) {
-    if (!a64 || !r64 || !rhs32 || !rraw32 || !mask32 || !a64->H || !a64->gamma) return GLIDE_E_NULL;
-    if (a64->dtype != GLIDE_F64) return GLIDE_E_DTYPE;
+    if (!a64 || !r64 || !rhs || !rraw || !mask || !a64->H || !a64->gamma) return GLIDE_E_NULL;
+    if (a64->dtype != GLIDE_F64 || (lin_dtype != GLIDE_F32 && lin_dtype != GLIDE_F64)) return GLIDE_E_DTYPE;
     const int64_t nb = a64->nb, ny = a64->ny, nx = a64->nx;
     const int64_t nf = nb * (ny * (nx + 1) + (ny + 1) * nx), nc = nb * ny * nx;
     glide::count_launch();
-    newton_rhs_k<<<nblocks(nf + nc), KB, 0, (cudaStream_t)stream>>>(
-        (float*)rhs32, (float*)rraw32, (float*)mask32, (const double*)r64, (const double*)a64->H,
-        (const double*)a64->gamma, a64->dt, nf, nc);
+    if (lin_dtype == GLIDE_F32)
+        newton_rhs_k<float><<<nblocks(nf + nc), KB, 0, (cudaStream_t)stream>>>(
+            (float*)rhs, (float*)rraw, (float*)mask, (const double*)r64, (const double*)a64->H,
+            (const double*)a64->gamma, a64->dt, nf, nc);
+    else
+        newton_rhs_k<double><<<nblocks(nf + nc), KB, 0, (cudaStream_t)stream>>>(
+            (double*)rhs, (double*)rraw, (double*)mask, (const double*)r64, (const double*)a64->H,
+            (const double*)a64->gamma, a64->dt, nf, nc);
     return (int)cudaGetLastError();
 }
 
@@ -203,15 +217,19 @@ int glide_active_mask(const GlideLevelArgs* a, const void* r_H, void* mask, void
     return (int)cudaGetLastError();
 }
 
-int glide_newton_update(const GlideLevelArgs* a64, void* U64, const void* base64, const void* d32, double alpha,
-                        void* stream) {
-    if (!a64 || !U64 || !base64 || !d32 || !a64->gamma) return GLIDE_E_NULL;
-    if (a64->dtype != GLIDE_F64) return GLIDE_E_DTYPE;
+int glide_newton_update(const GlideLevelArgs* a64, void* U64, const void* base64, const void* d, int d_dtype,
+                        double alpha, void* stream) {
+    if (!a64 || !U64 || !base64 || !d || !a64->gamma) return GLIDE_E_NULL;
+    if (a64->dtype != GLIDE_F64 || (d_dtype != GLIDE_F32 && d_dtype != GLIDE_F64)) return GLIDE_E_DTYPE;
     const int64_t nb = a64->nb, ny = a64->ny, nx = a64->nx;
     const int64_t nf = nb * (ny * (nx + 1) + (ny + 1) * nx), nc = nb * ny * nx;
     glide::count_launch();
-    newton_update_k<<<nblocks(nf + nc), KB, 0, (cudaStream_t)stream>>>(
-        (double*)U64, (const double*)base64, (const float*)d32, alpha, (const double*)a64->gamma, nf, nc);
+    if (d_dtype == GLIDE_F32)
+        newton_update_k<float><<<nblocks(nf + nc), KB, 0, (cudaStream_t)stream>>>(
+            (double*)U64, (const double*)base64, (const float*)d, alpha, (const double*)a64->gamma, nf, nc);
+    else
+        newton_update_k<double><<<nblocks(nf + nc), KB, 0, (cudaStream_t)stream>>>(
+            (double*)U64, (const double*)base64, (const double*)d, alpha, (const double*)a64->gamma, nf, nc);
     return (int)cudaGetLastError();
 }
 

@@ -1,5 +1,7 @@
 // BF16 tensor-core GEMM on the 5th-generation tensor cores (tcgen05 + TMEM)
-// for the learned initial guess (3x3 convolutions as im2col GEMMs).
+// for the learned initial guess: 3x3 convolutions as GEMMs, either on an
+// explicit im2col matrix (training, whose weight gradient needs it) or with
+// the im2col done while staging the A tile (inference, no im2col buffer).
 //
 //   C[M,N] (+)= A[M,K] * B[N,K]^T   (A, B: BF16, K-major; accumulate FP32 in TMEM)
 //   epilogue: + bias[N], ReLU, store FP32 or BF16, or add into FP32 C.
@@ -97,12 +99,42 @@ __device__ __forceinline__ void stage_tile(uint8_t* s, const __nv_bfloat16* __re
     }
 }
 
-// out_mode: 0 = store FP32, 1 = store BF16, 2 = add into FP32
+// Implicit im2col of a 3x3 "same" convolution: rows [m0, m0+GM) of the A
+// operand are output pixels p = (b*H + y)*W + x of an NHWC BF16 input
+// (C a multiple of 8, so each 16-byte chunk of a row lies in one tap), column
+// k = (ky*3 + kx)*C + c holds x[b, y+ky-1, x+kx-1, c] (zero outside).  The
+// staged tile is the one stage_tile would read from the explicit im2col
+// matrix, so the products are bit-identical.
+struct ConvShape {
+    int Bn, H, W, C;
+};
+__device__ __forceinline__ void stage_tile_conv(uint8_t* s, const __nv_bfloat16* __restrict__ x, const ConvShape cs,
+                                                int M, int K, int m0, int k0) {
+    for (int idx = threadIdx.x; idx < GM * (GK / 8); idx += GTHREADS) {
+        const int row = idx / (GK / 8), kc = idx % (GK / 8);
+        const int p = m0 + row, k = k0 + kc * 8;
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (p < M && k < K) {
+            const int tap = k / cs.C, c = k - tap * cs.C;
+            const int ky = tap / 3, kx = tap - 3 * ky;
+            const int xx = p % cs.W, t = p / cs.W;
+            const int yy = t % cs.H, b = t / cs.H;
+            const int sy = yy + ky - 1, sx = xx + kx - 1;
+            if (sy >= 0 && sy < cs.H && sx >= 0 && sx < cs.W)
+                val = *reinterpret_cast<const uint4*>(x + ((int64_t(b) * cs.H + sy) * cs.W + sx) * cs.C + c);
+        }
+        *reinterpret_cast<uint4*>(s + tile_off(row, kc)) = val;
+    }
+}
+
+// out_mode: 0 = store FP32, 1 = store BF16, 2 = add into FP32.  CONV: A is the
+// NHWC input of a 3x3 convolution read through stage_tile_conv (lda unused).
+template <bool CONV>
 __global__ void __launch_bounds__(GTHREADS) tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, int lda,
                                                            const __nv_bfloat16* __restrict__ B, int ldb, void* C,
                                                            int ldc, int M, int N, int K,
                                                            const float* __restrict__ bias, int relu, int out_mode,
-                                                           int* err) {
+                                                           int* err, ConvShape cs) {
     __shared__ __align__(1024) uint8_t sA[GM * GK * 2];
     __shared__ __align__(1024) uint8_t sB[GN * GK * 2];
     __shared__ __align__(8) uint64_t mbar;
@@ -133,7 +165,10 @@ __global__ void __launch_bounds__(GTHREADS) tc_gemm_kernel(const __nv_bfloat16* 
     const int nchunks = (K + GK - 1) / GK;
     for (int ch = 0; ch < nchunks && ok; ch++) {
         const int k0 = ch * GK;
-        stage_tile<GM>(sA, A, M, K, lda, m0, k0);
+        if (CONV)
+            stage_tile_conv(sA, A, cs, M, K, m0, k0);
+        else
+            stage_tile<GM>(sA, A, M, K, lda, m0, k0);
         stage_tile<GN>(sB, B, N, K, ldb, n0, k0);
         // make the generic-proxy smem writes visible to the tensor core (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -212,7 +247,25 @@ extern "C" int glide_gemm_bf16(const void* A, int lda, const void* B, int ldb, v
     if (!A || !B || !C) return GLIDE_E_NULL;
     if (M < 1 || N < 1 || K < 1 || lda < K || ldb < K || ldc < N || out_mode < 0 || out_mode > 2) return GLIDE_E_SHAPE;
     dim3 grid((M + glide::GM - 1) / glide::GM, (N + glide::GN - 1) / glide::GN);
-    glide::count_launch(), glide::tc_gemm_kernel<<<grid, glide::GTHREADS, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err);
+    glide::count_launch(), glide::tc_gemm_kernel<false><<<grid, glide::GTHREADS, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err,
+        glide::ConvShape{0, 0, 0, 0});
+    return (int)cudaGetLastError();
+}
+
+extern "C" int glide_conv3x3_bf16(const void* x, int Bn, int H, int W, int C, const void* Wt, int ldw, void* out,
+                                  int ldc, int N, const float* bias, int relu, int out_mode, int* err, void* stream) {
+    if (!x || !Wt || !out) return GLIDE_E_NULL;
+    if (Bn < 1 || H < 1 || W < 1 || C < 8 || C % 8 != 0 || N < 1 || ldw < 9 * C || ldc < N || out_mode < 0 ||
+        out_mode > 2)
+        return GLIDE_E_SHAPE;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) != 0) return GLIDE_E_SHAPE;
+    const int64_t M64 = int64_t(Bn) * H * W;
+    if (M64 >= (int64_t(1) << 31)) return GLIDE_E_TOO_LARGE;
+    const int M = int(M64), K = 9 * C;
+    dim3 grid((M + glide::GM - 1) / glide::GM, (N + glide::GN - 1) / glide::GN);
+    glide::count_launch(), glide::tc_gemm_kernel<true><<<grid, glide::GTHREADS, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)x, 0, (const __nv_bfloat16*)Wt, ldw, out, ldc, M, N, K, bias, relu, out_mode, err,
+        glide::ConvShape{Bn, H, W, C});
     return (int)cudaGetLastError();
 }

@@ -9,7 +9,8 @@ of FAS V-cycles and never solves to a tolerance.  Once the FAS phase of
    on); cells with H - dt r_H <= gamma (the Vanka smoother's rule) form the
    active set, whose rows become the constraint H - gamma
    (``glide_newton_rhs``);
-2. solves J(fl32 U) d = -r in FP32 with FGMRES(m) to a relative tolerance,
+2. solves J(fl32 U) d = -r in FP32 (or J(U) d = -r in FP64 on the FP64
+   path) with FGMRES(m) to a relative tolerance,
    right-preconditioned by one linear multigrid V-cycle per iteration
    (``glide_linear_vcycle``, replayed from a CUDA graph): linear Vanka sweeps
    on every level with the local matrices factored once per step, each coarse
@@ -19,8 +20,9 @@ of FAS V-cycles and never solves to a tolerance.  Once the FAS phase of
    FP64 dot products (``glide_dots``/``glide_combine``);
 3. sets U += alpha fl64(d) with H >= gamma, halving alpha until |r| falls.
 
-The FP32 correction's rounding error scales with d, not with the operator's
-terms, so the steps converge to the FP64 solution (iterative refinement).
+In the mixed path the FP32 correction's rounding error scales with d, not
+with the operator's terms, so the steps converge to the FP64 solution
+(iterative refinement).
 """
 from __future__ import annotations
 
@@ -34,18 +36,25 @@ from . import _native as N
 
 
 class NewtonKrylov:
+    """The Newton-Krylov finish of one IcePhysics object.  With
+    ``precision="mixed"`` the linear solves run on the FP32 hierarchy (FP32
+    corrections of the FP64 state); with ``precision="fp64"`` on the FP64
+    hierarchy itself (level 0's state is then the state being corrected)."""
+
     def __init__(self, physics, m=20):
         self.ph = physics
         self.lib = N.load()
-        self.gs = physics.grids32
+        self.mixed = physics.grid32 is not None
+        self.gs = physics.grids32 if self.mixed else physics.grids
         g0 = self.gs[0]
         self.n = g0.nb * g0.n_total
         self.m = int(m)
         dev = g0.device
-        self.V = torch.zeros(self.m + 1, self.n, dtype=torch.float32, device=dev)
-        self.Z = torch.zeros(self.m, self.n, dtype=torch.float32, device=dev)
-        self.w = torch.zeros(self.n, dtype=torch.float32, device=dev)
-        self.x = torch.zeros(self.n, dtype=torch.float32, device=dev)
+        self.dtype, self.code = g0.dtype, g0.code
+        self.V = torch.zeros(self.m + 1, self.n, dtype=self.dtype, device=dev)
+        self.Z = torch.zeros(self.m, self.n, dtype=self.dtype, device=dev)
+        self.w = torch.zeros(self.n, dtype=self.dtype, device=dev)
+        self.x = torch.zeros(self.n, dtype=self.dtype, device=dev)
         self.hb = torch.zeros(2 * self.m + 4, dtype=torch.float64, device=dev)
         self.y = torch.zeros(self.m, dtype=torch.float64, device=dev)
         self.parts = torch.zeros(self.lib.glide_dots_parts(self.n) * 32, dtype=torch.float64, device=dev)
@@ -99,15 +108,15 @@ class NewtonKrylov:
             pass
 
     def _dots(self, V, k, w, out):
-        N.check(self.lib.glide_dots(N.F32, self.n, k, V.data_ptr(), self.n, w.data_ptr(), out.data_ptr(),
+        N.check(self.lib.glide_dots(self.code, self.n, k, V.data_ptr(), self.n, w.data_ptr(), out.data_ptr(),
                                     self.parts.data_ptr(), self._s()), "dots")
 
     def _combine(self, V, k, coef, alpha, out, beta):
-        N.check(self.lib.glide_combine(N.F32, self.n, k, V.data_ptr(), self.n, coef.data_ptr(), float(alpha),
+        N.check(self.lib.glide_combine(self.code, self.n, k, V.data_ptr(), self.n, coef.data_ptr(), float(alpha),
                                        out.data_ptr(), float(beta), self._s()), "combine")
 
     def _scale(self, out, x, a):
-        N.check(self.lib.glide_lincomb(N.F32, out.data_ptr(), x.data_ptr(), float(a), None, 0.0, self.n, self._s()),
+        N.check(self.lib.glide_lincomb(self.code, out.data_ptr(), x.data_ptr(), float(a), None, 0.0, self.n, self._s()),
                 "lincomb")
 
     # ------------------------------------------------------------------ FGMRES
@@ -211,8 +220,9 @@ class NewtonKrylov:
             g64.gamma.fill_(ph.thklim)
             g64.compute_residual()
             N.check(lib.glide_newton_rhs(C.byref(a64), g64.r.data_ptr(), buf["lin_rhs"].data_ptr(),
-                                         buf["r_raw"].data_ptr(), buf["mask"].data_ptr(), s), "newton rhs")
-            N.check(lib.glide_convert(N.F32, g0.U.data_ptr(), g64.U.data_ptr(), ntot, 0, s), "convert")
+                                         buf["r_raw"].data_ptr(), buf["mask"].data_ptr(), self.code, s), "newton rhs")
+            if self.mixed:
+                N.check(lib.glide_convert(N.F32, g0.U.data_ptr(), g64.U.data_ptr(), ntot, 0, s), "convert")
             N.check(lib.glide_linear_setup(arr, nlev, C.byref(cfg), s), "linear setup")
             # forcing term: no more accuracy than the step needs (Newton converges fast here)
             eta = min(0.5, max(rtol, 0.3 * tol / rel))
@@ -224,7 +234,7 @@ class NewtonKrylov:
             alpha, accepted = 1.0, False
             for _ in range(max_ls):
                 N.check(lib.glide_newton_update(C.byref(a64), g64.U.data_ptr(), self.base.data_ptr(),
-                                                self.x.data_ptr(), alpha, s), "newton update")
+                                                self.x.data_ptr(), self.code, alpha, s), "newton update")
                 new = ph.residual_norm() / r0
                 if math.isfinite(new) and new < rel:
                     accepted = True

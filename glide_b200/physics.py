@@ -177,8 +177,8 @@ class IcePhysics:
         self.finish_patience = int(finish_patience)
         self.finish_fas_until = float(finish_fas_until)
         self.finish_fas_patience = int(finish_fas_patience)
-        if newton and precision != "mixed":
-            raise ValueError('newton=True needs precision="mixed" (FP32 corrections of an FP64 state)')
+        if newton and precision == "fp32":
+            raise ValueError('newton=True needs an FP64 state: precision="mixed" or "fp64"')
         self.newton = bool(newton)
         self.newton_start = float(newton_start)
         self.newton_max_steps = int(newton_max_steps)

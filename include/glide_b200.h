@@ -241,14 +241,15 @@ int glide_linear_vcycle(GlideLevel* levels, int n_levels, const GlideSolverConfi
 int glide_vanka_lu_masked(const GlideLevelArgs* a, void* lu, double shift, void* stream);
 /* Newton step helpers (no counterpart in the reference).  glide_newton_rhs:
  * from the FP64 residual r (monolithic, faces then cells) of the FP64 level
- * a64, the active set H - dt r_H <= gamma into mask32 (cells) and the FP32
- * right-hand side rhs32 (r with active rows replaced by H - gamma) and
- * rraw32 = fl32(r).  glide_newton_update: U64 = base64 + alpha * fl64(d32)
- * with H kept >= gamma.  glide_active_mask: mask = (H - dt r_H <= gamma). */
-int glide_newton_rhs(const GlideLevelArgs* a64, const void* r64, void* rhs32, void* rraw32, void* mask32,
+ * a64, the active set H - dt r_H <= gamma into mask (cells), the right-hand
+ * side rhs (r with active rows replaced by H - gamma) and rraw = r, all three
+ * in lin_dtype (GLIDE_F32 for the mixed path, GLIDE_F64 for the FP64 path).
+ * glide_newton_update: U64 = base64 + alpha * d (d of d_dtype) with H kept
+ * >= gamma.  glide_active_mask: mask = (H - dt r_H <= gamma). */
+int glide_newton_rhs(const GlideLevelArgs* a64, const void* r64, void* rhs, void* rraw, void* mask, int lin_dtype,
                      void* stream);
-int glide_newton_update(const GlideLevelArgs* a64, void* U64, const void* base64, const void* d32, double alpha,
-                        void* stream);
+int glide_newton_update(const GlideLevelArgs* a64, void* U64, const void* base64, const void* d, int d_dtype,
+                        double alpha, void* stream);
 int glide_active_mask(const GlideLevelArgs* a, const void* r_H, void* mask, void* stream);
 /* out[i] = sum_j V[i*ldv + j] * w[j], i < k <= 32, FP64 accumulation in a fixed
  * order (deterministic); out: k device doubles; parts: glide_dots_parts(n) * k
@@ -292,6 +293,14 @@ int glide_loss_parts(int64_t n);
  * null) is set to 1 if a tensor-core wait ran out (the tile is then skipped). */
 int glide_gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
                     const float* bias, int relu, int out_mode, int* err, void* stream);
+/* 3x3 "same" convolution as an implicit GEMM on the tcgen05 tensor cores:
+ * out[Bn*H*W, N] (+)= im2col(x) * Wt^T with x NHWC BF16 (C a multiple of 8,
+ * 16-byte aligned), Wt (N, ldw >= 9C) BF16 with K = (ky*3+kx)*C + c, the
+ * im2col gathered while staging each A tile (no col buffer); epilogue and
+ * err as glide_gemm_bf16.  Bit-identical to glide_im2col3_bf16 followed by
+ * glide_gemm_bf16 with Kp = 9C. */
+int glide_conv3x3_bf16(const void* x, int Bn, int H, int W, int C, const void* Wt, int ldw, void* out, int ldc, int N,
+                       const float* bias, int relu, int out_mode, int* err, void* stream);
 /* im2col of a 3x3 same convolution on NHWC BF16 x (Bn,H,W,C) into col (Bn*H*W, Kp), Kp >= 9C (zero pad). */
 int glide_im2col3_bf16(const void* x, void* col, int Bn, int H, int W, int C, int Kp, void* stream);
 /* Transpose of im2col (gather form): dx (Bn,H,W,C) FP32 from dcol (Bn*H*W, Kp) FP32. */

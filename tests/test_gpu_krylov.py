@@ -9,7 +9,10 @@
 * the linear V-cycle (glide_linear_vcycle) cuts the linear residual
   |g + J d| / |g| on a dome state, and its CUDA-graph replay equals the eager
   call bit for bit;
-* the Anderson step's native products equal torch FP64 products.
+* the Anderson step's native products equal torch FP64 products;
+* the Newton-Krylov finish on the mixed and on the FP64 path takes Newton
+  steps and reaches |r|/|r0| <= 1e-9 on the 128^2 dome, judged by the FP64
+  oracle's own residual.
 """
 import ctypes as C
 
@@ -77,7 +80,8 @@ def test_newton_rhs_and_update():
     mask = torch.zeros(g.ny, g.nx, dtype=torch.float32, device="cuda")
     a = g.level_args()
     s = torch.cuda.current_stream().cuda_stream
-    assert lib.glide_newton_rhs(C.byref(a), g.r.data_ptr(), rhs.data_ptr(), rraw.data_ptr(), mask.data_ptr(), s) == 0
+    assert lib.glide_newton_rhs(C.byref(a), g.r.data_ptr(), rhs.data_ptr(), rraw.data_ptr(), mask.data_ptr(), N.F32,
+                                s) == 0
     act = (g.H - g.dt * g.r_H <= g.gamma)
     assert torch.equal(mask, act.float())
     ref = g.r.clone()
@@ -86,7 +90,7 @@ def test_newton_rhs_and_update():
     assert torch.equal(rraw, g.r.float())
     d = torch.randn(n, device="cuda", dtype=torch.float32) * 10
     base = g.U.clone()
-    assert lib.glide_newton_update(C.byref(a), g.U.data_ptr(), base.data_ptr(), d.data_ptr(), 0.5, s) == 0
+    assert lib.glide_newton_update(C.byref(a), g.U.data_ptr(), base.data_ptr(), d.data_ptr(), N.F32, 0.5, s) == 0
     ref = base + 0.5 * d.double()
     ref[nU:] = torch.maximum(ref[nU:], g.gamma.flatten())
     assert torch.equal(g.U, ref)
@@ -137,7 +141,7 @@ def test_linear_vcycle_reduces_linear_residual_and_replays():
     a64 = g64.level_args()
     g64.compute_residual()
     assert lib.glide_newton_rhs(C.byref(a64), g64.r.data_ptr(), buf["lin_rhs"].data_ptr(), buf["r_raw"].data_ptr(),
-                                buf["mask"].data_ptr(), s) == 0
+                                buf["mask"].data_ptr(), N.F32, s) == 0
     assert lib.glide_convert(N.F32, g0.U.data_ptr(), g64.U.data_ptr(), g64.n_total, 0, s) == 0
     assert lib.glide_linear_setup(arr, nlev, C.byref(cfg), s) == 0
     assert lib.glide_linear_vcycle(arr, nlev, C.byref(cfg), s) == 0
@@ -170,3 +174,27 @@ def test_anderson_native_products_match_torch():
     coef = np.array([0.5, -1.0, 2.0, 0.25])
     p.combine(rows, coef, out)
     assert torch.allclose(out, rows.T @ torch.as_tensor(coef, device="cuda"), rtol=1e-13, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_newton_krylov_finish_reaches_tolerance(precision):
+    import bench
+    from glide_b200 import IcePhysics
+    from glide_b200.synthetic import dome_case
+    from oracle.check import relative_residuals
+    c = dome_case(2, n=128, dx=2500.0, n_levels=4)
+    kw = dict(bench.FAST_KW if precision == "mixed" else bench.FP64_FAST_KW)
+    kw.update(newton=True, newton_start=1e-1, newton_after=0, newton_min_gain=1.0, newton_local=2,
+              newton_max_steps=12)
+    ph = IcePhysics(128, 128, c.dx, n_levels=4, thklim=c.thklim, precision=precision,
+                    settings=bench.fast_settings(), **kw)
+    ph.set_geometry(c.bed, c.thickness)
+    ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
+    u, v, H = ph.forward(c.dt, tol=1e-9, max_vcycles=40, max_finish_sweeps=20000, update_geometry=False)
+    info = ph.last_info
+    assert info["newton_steps"] >= 1, info
+    assert info["rel_residual"] <= 1e-9, info
+    geo = dict(bed=c.bed, B=c.B, beta=c.beta, H_prev=c.thickness, smb=c.smb, dx=c.dx, dt=c.dt, thklim=c.thklim)
+    state = tuple(t.detach().double().cpu().numpy() for t in (u, v, H))
+    orc = relative_residuals([(geo, [state])], workers=1)[0][0]
+    assert orc <= 1.05e-9, (orc, info)

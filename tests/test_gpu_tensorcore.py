@@ -97,3 +97,23 @@ def test_transpose():
     assert lib.glide_transpose_bf16(x.data_ptr(), y.data_ptr(), 70, 45, torch.cuda.current_stream().cuda_stream) == 0
     torch.cuda.synchronize()
     assert torch.equal(y, x.T)
+
+
+@pytest.mark.parametrize("C_in,C_out,out_mode", [(8, 32, 1), (32, 64, 1), (96, 32, 0), (64, 128, 1)])
+def test_implicit_conv3x3_equals_im2col_gemm(C_in, C_out, out_mode):
+    """glide_conv3x3_bf16 (im2col gathered while staging each tile) against
+    glide_im2col3_bf16 + glide_gemm_bf16 on the same inputs: the staged tiles
+    are the same, so the results are bit-identical (ragged M and N edges,
+    zero padding at the image border, bias and ReLU in the epilogue)."""
+    from glide_b200.guess import conv3x3, gemm as lib_gemm, im2col3
+    g = torch.Generator(device="cuda").manual_seed(C_in + C_out)
+    x = torch.randn(2, 37, 45, C_in, generator=g, device="cuda").to(torch.bfloat16)
+    Wb = (torch.randn(C_out, 9 * C_in, generator=g, device="cuda") * 0.1).to(torch.bfloat16)
+    bias = torch.randn(C_out, generator=g, device="cuda")
+    dt = torch.bfloat16 if out_mode == 1 else torch.float32
+    a = torch.empty((2 * 37 * 45, C_out), dtype=dt, device="cuda")
+    b = torch.empty_like(a)
+    lib_gemm(im2col3(x), Wb, a, bias=bias, relu=True, out_mode=out_mode)
+    conv3x3(x, Wb, b, bias=bias, relu=True, out_mode=out_mode)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
