@@ -1,7 +1,8 @@
 """Build ``oracle/_ref/libglide_ref.so`` from the reference's CUDA sources.
 
 Test infrastructure: compiles the reference kernels where they lie
-(``<reference>/glide/cuda/*.cu``) together with the host launchers in
+(``<reference>/glide/cuda/*.cu``; ``<reference>`` is ``$GLIDE_REFERENCE``, else
+the ``reference`` directory beside this repository) together with the host launchers in
 ``oracle/ref_ice_shim.cu`` / ``oracle/ref_util_shim.cu``.  The ice kernels get
 ``--use_fast_math`` like the reference's NVRTC build (glide/kernels.py:72);
 the transfer kernels do not (glide/kernels.py:63).  Outputs go to
@@ -17,7 +18,9 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 LIB = OUT / "libglide_ref.so"
-REF_CUDA = Path(os.environ.get("GLIDE_REFERENCE", "/root/reference")) / "glide" / "cuda"
+# the reference checkout: GLIDE_REFERENCE, else a "reference" directory beside this repository
+REF_ROOT = Path(os.environ.get("GLIDE_REFERENCE", HERE.parent.parent / "reference"))
+REF_CUDA = REF_ROOT / "glide" / "cuda"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

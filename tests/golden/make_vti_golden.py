@@ -1,7 +1,7 @@
 """Golden VTI file from the reference's own writer (glide/io.py:20-137).
 
-Run in a container that has the reference tree (path in GLIDE_REFERENCE,
-default /root/reference).  CuPy and h5py are absent there, so ``glide/io.py`` is
+Run where the reference tree is present (path in GLIDE_REFERENCE, else the
+``reference`` directory beside this repository).  CuPy and h5py are absent there, so ``glide/io.py`` is
 loaded with stand-in ``cupy`` (``asnumpy`` = ``numpy.asarray``; the writer
 only moves arrays to the host with it) and ``h5py`` (empty; only the HDF5
 writer, not exercised here, uses it) modules.  Writes
@@ -26,7 +26,7 @@ def vti_fields():
 
 
 def main():
-    ref = Path(os.environ.get("GLIDE_REFERENCE", "/root/reference")) / "glide" / "io.py"
+    ref = Path(os.environ.get("GLIDE_REFERENCE", HERE.parents[2] / "reference")) / "glide" / "io.py"
     cp = types.ModuleType("cupy")
     cp.asnumpy = np.asarray
     sys.modules.setdefault("cupy", cp)
