@@ -66,7 +66,7 @@ class SolverConfig(C.Structure):
                 ("adj_omega", C.c_double), ("exact_adjoint", C.c_int), ("smooth_H_correction", C.c_int),
                 ("newton_step", C.c_double), ("pivoted_lu", C.c_int), ("coarse_line_search", C.c_int),
                 ("lin_pre", C.c_int), ("lin_post", C.c_int), ("lin_coarse", C.c_int), ("lin_omega", C.c_double),
-                ("lin_shift", C.c_double)]
+                ("lin_shift", C.c_double), ("adj_active_tol", C.c_double)]
 
 
 class NativeError(RuntimeError):

@@ -11,7 +11,8 @@ V-cycle (glide/solver.py:160-220) on the kernels of this package:
 
 The last term follows from f_H = H_prev/dt + smb (glide/physics.py:173); it
 is new here (the reference adjoint returns grad_beta only).  Rows of cells
-held at the thickness limit (mask m: H <= gamma + 0.1, glide/grid.py:332)
+held at the thickness limit (mask m: H <= gamma + 0.1 by default,
+``SolverSettings.adj_active_tol``; glide/grid.py:332)
 are identity rows of J, so they pass no sensitivity to H_prev.
 
 ``TimeStepper`` chains n steps; its backward recomputes each segment of
@@ -68,7 +69,7 @@ def _restore(physics, beta, H_prev, U, dt):
 def _adjoint(physics, du, dv, dH, dt, adj_tol, max_vcycles):
     g = physics.grid
     grad_beta = physics.adjoint(du, dv, dH, tol=adj_tol, max_vcycles=max_vcycles, exact=True)
-    g.compute_mask()
+    g.compute_mask(physics.settings.adj_active_tol)
     grad_Hprev = -(1.0 - g.mask) * g.lambda_H / dt
     g.mask.zero_()
     return grad_beta.clone(), grad_Hprev.clone()

@@ -420,9 +420,10 @@ int fascd(GlideLevel* lv, int n, int k, bool finest, const GlideSolverConfig* c,
     return fill_gamma(L, c->thklim, s);
 }
 
-int mask_on(GlideLevel* L, void* s) {
+int mask_on(GlideLevel* L, const GlideSolverConfig* c, void* s) {
     LevelView w = view(L);
-    return glide_mask_le(w.dt, (void*)L->a.mask, L->a.H, L->a.gamma, 0.1, w.nc * w.nb, s);
+    const double tol = c->adj_active_tol > 0.0 ? c->adj_active_tol : 0.1;   // glide/grid.py:332-334
+    return glide_mask_le(w.dt, (void*)L->a.mask, L->a.H, L->a.gamma, tol, w.nc * w.nb, s);
 }
 int mask_off(GlideLevel* L, void* s) {
     LevelView w = view(L);
@@ -464,13 +465,13 @@ int adjoint(GlideLevel* lv, int n, int k, const GlideSolverConfig* c, void* s) {
     LevelView w = view(L);
     const int ex = c->exact_adjoint;
     if (k == n - 1) {
-        TRY(mask_on(L, s));
+        TRY(mask_on(L, c, s));
         TRY(vanka_adj(L, c->adj_coarse, c->adj_omega, ex, s));
         return mask_off(L, s);
     }
     GlideLevel* C = &lv[k + 1];
     LevelView wc = view(C);
-    TRY(mask_on(L, s));
+    TRY(mask_on(L, c, s));
     TRY(vanka_adj(L, c->adj_smooth, c->adj_omega, ex, s));
     TRY(mask_off(L, s));
     TRY(adj_residual(L, ex, s));                               // solver.py:187-189 (mask = 0)
@@ -481,7 +482,7 @@ int adjoint(GlideLevel* lv, int n, int k, const GlideSolverConfig* c, void* s) {
     TRY(glide_prolong(w.dt, 0, 1, 1, wc.u(C->lam), w.u(L->lam), C->a.ny, C->a.nx, C->a.nb, s));
     TRY(glide_prolong(w.dt, 1, 1, 1, wc.v(C->lam), w.v(L->lam), C->a.ny, C->a.nx, C->a.nb, s));
     TRY(glide_prolong(w.dt, 2, 1, 1, wc.H(C->lam), w.H(L->lam), C->a.ny, C->a.nx, C->a.nb, s));
-    TRY(mask_on(L, s));
+    TRY(mask_on(L, c, s));
     TRY(vanka_adj(L, c->adj_smooth, c->adj_omega, ex, s));
     return mask_off(L, s);
 }

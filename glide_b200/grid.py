@@ -287,10 +287,10 @@ class Grid:
         N.check(self._lib.glide_mask_le(self.code, self.mask.data_ptr(), self.H.data_ptr(), self.gamma.data_ptr(),
                                         float(tol), self.nb * self.nh, self._s()), "mask")
 
-    def compute_grad_beta(self, exact_boundary=False):
+    def compute_grad_beta(self, exact_boundary=False, mask_tol=1e-1):
         """grad_beta from the current Lambda (glide/grid.py:336-355)."""
         grad = self._cells()
-        self.compute_mask()
+        self.compute_mask(mask_tol)
         a = self.level_args()
         N.check(self._lib.glide_grad_beta(C.byref(a), self.lambda_u.data_ptr(), self.lambda_v.data_ptr(),
                                           grad.data_ptr(), int(exact_boundary), self._s()), "grad beta")

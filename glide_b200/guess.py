@@ -10,9 +10,11 @@ Network: 4 resolution levels, 32 base channels (32-64-128-256), two 3x3
 conv + ReLU per level, 2x average pooling down, nearest upsampling and skip
 concatenation up, a 1x1 head to 2 channels.  Activations are NHWC BF16,
 weights are kept in FP32 for the optimiser and cast to BF16 for the
-products.  Every convolution (forward, data gradient, weight gradient) runs
-as im2col + the tcgen05 BF16 GEMM with FP32 accumulation in TMEM
-(``glide_gemm_bf16``); bias and ReLU are fused into the GEMM epilogue.
+products.  Every convolution runs on the tcgen05 BF16 GEMM with FP32
+accumulation in TMEM: in training (forward, data gradient, weight gradient)
+as im2col + ``glide_gemm_bf16``, in inference as an implicit GEMM that
+gathers the im2col rows while staging each tile (``glide_conv3x3_bf16``);
+bias and ReLU are fused into the GEMM epilogue.
 Pooling, upsampling, concatenation and the optimiser are element-wise torch
 glue.  This part has no counterpart in the reference.
 """
@@ -44,6 +46,10 @@ def _lib():
         lib.glide_col2im3_f32.restype = C.c_int
         lib.glide_transpose_bf16.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         lib.glide_transpose_bf16.restype = C.c_int
+        lib.glide_conv3x3_bf16.argtypes = [C.c_void_p] + [C.c_int] * 4 + [C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                                                          C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                                                          C.c_void_p, C.c_void_p]
+        lib.glide_conv3x3_bf16.restype = C.c_int
         lib._guess_sigs = True
     return lib
 
@@ -72,6 +78,20 @@ def gemm(A, B, out, bias=None, relu=False, out_mode=0):
     return out
 
 
+def conv3x3(x, Wb, out, bias=None, relu=False, out_mode=1):
+    """out (+)= conv3x3(x) on the tensor cores as an implicit GEMM (no im2col
+    buffer): x NHWC BF16 with C % 8 == 0, Wb (Cout, 9C) BF16."""
+    assert x.dtype == torch.bfloat16 and Wb.dtype == torch.bfloat16
+    assert x.is_contiguous() and Wb.is_contiguous() and out.is_contiguous()
+    Bn, H, W, Cc = x.shape
+    Nn = Wb.shape[0]
+    rc = _lib().glide_conv3x3_bf16(x.data_ptr(), Bn, H, W, Cc, Wb.data_ptr(), Wb.shape[1], out.data_ptr(), Nn, Nn,
+                                   None if bias is None else bias.data_ptr(), int(relu), int(out_mode),
+                                   _err_flag(x.device).data_ptr(), N.stream_handle())
+    N.check(rc, "tensor-core conv3x3")
+    return out
+
+
 def im2col3(x):
     Bn, H, W, Cc = x.shape
     col = torch.empty((Bn * H * W, 9 * Cc), dtype=torch.bfloat16, device=x.device)
@@ -95,6 +115,20 @@ def transpose(x):
     return y
 
 
+def conv3x3_relu(x, W, b, relu=True):
+    """relu(conv3x3(x, W) + b).  With autograd recording (training) this is
+    Conv3x3ReLU, which keeps the im2col matrix for the weight gradient; without
+    (inference) the im2col is gathered inside the GEMM when Cin % 8 == 0, with a
+    bit-identical result."""
+    Bn, H, Wd, Cin = x.shape
+    if (torch.is_grad_enabled() and (x.requires_grad or W.requires_grad or b.requires_grad)) or Cin % 8 != 0:
+        return Conv3x3ReLU.apply(x, W, b, relu)
+    Cout = W.shape[0]
+    y = torch.empty((Bn * H * Wd, Cout), dtype=torch.bfloat16, device=x.device)
+    conv3x3(x.contiguous(), W.detach().to(torch.bfloat16).contiguous(), y, bias=b.detach(), relu=relu, out_mode=1)
+    return y.view(Bn, H, Wd, Cout)
+
+
 class Conv3x3ReLU(torch.autograd.Function):
     """y = relu(conv3x3(x, W) + b); x NHWC BF16, W (Cout, 9*Cin) FP32 master."""
 
@@ -103,9 +137,9 @@ class Conv3x3ReLU(torch.autograd.Function):
         Bn, H, Wd, Cin = x.shape
         Cout = W.shape[0]
         x = x.contiguous()
-        col = im2col3(x)
         Wb = W.to(torch.bfloat16).contiguous()
         y = torch.empty((Bn * H * Wd, Cout), dtype=torch.bfloat16, device=x.device)
+        col = im2col3(x)
         gemm(col, Wb, y, bias=b, relu=relu, out_mode=1)
         ctx.save_for_backward(col, Wb, y)
         ctx.shape = (Bn, H, Wd, Cin)
@@ -206,15 +240,15 @@ class UNet(torch.nn.Module):
         i = 0
         skips = []
         for k in range(self.levels):
-            x = Conv3x3ReLU.apply(x, self.ws[i], self.bs[i], True); i += 1
-            x = Conv3x3ReLU.apply(x, self.ws[i], self.bs[i], True); i += 1
+            x = conv3x3_relu(x, self.ws[i], self.bs[i]); i += 1
+            x = conv3x3_relu(x, self.ws[i], self.bs[i]); i += 1
             if k < self.levels - 1:
                 skips.append(x)
                 x = _pool(x)
         for k in range(self.levels - 2, -1, -1):
             x = torch.cat([_up(x), skips[k]], dim=3)
-            x = Conv3x3ReLU.apply(x, self.ws[i], self.bs[i], True); i += 1
-            x = Conv3x3ReLU.apply(x, self.ws[i], self.bs[i], True); i += 1
+            x = conv3x3_relu(x, self.ws[i], self.bs[i]); i += 1
+            x = conv3x3_relu(x, self.ws[i], self.bs[i]); i += 1
         return Conv1x1.apply(x, self.head_w, self.head_b)
 
     def flops(self, H, W):

@@ -256,3 +256,205 @@ class NewtonKrylov:
         info["newton_steps"] = info.get("newton_steps", 0) + steps
         info["krylov_its"] = info.get("krylov_its", 0) + its_total
         return rel
+
+
+class AdjointKrylov:
+    """FGMRES(m) for the adjoint system of a solved step,
+
+        J_m(U)^T lam = f_adj,
+
+    J_m: the Jacobian of F(U) - f with the rows of the active cells
+    (H <= gamma + adj_active_tol) replaced by the identity, the system the
+    reference's adjoint V-cycle relaxes (glide/solver.py:160-220,
+    glide/grid.py:319-334).  Right-preconditioned by one adjoint V-cycle per
+    iteration (``glide_adjoint_vcycle`` from lam = 0, replayed from a CUDA
+    graph; on the FP32 hierarchy in the mixed path, its input and output
+    converted).  The Krylov vectors, the operator (``glide_vjp``) and the
+    residual it reports are in the state's precision, so the mixed path's
+    multiplier solves the FP64 system.  No counterpart in the reference, which
+    runs two adjoint V-cycles (glide/physics.py:211-242)."""
+
+    def __init__(self, physics, m=30):
+        self.ph = physics
+        self.lib = N.load()
+        g = physics.grid
+        self.mixed = physics.grid32 is not None
+        self.gc = physics.grid32 if self.mixed else g   # level 0 of the cycle hierarchy
+        self.n = g.nb * g.n_total
+        self.m = int(m)
+        dev, dt = g.device, g.dtype
+        self.code = g.code
+        self.V = torch.zeros(self.m + 1, self.n, dtype=dt, device=dev)
+        self.Z = torch.zeros(self.m, self.n, dtype=dt, device=dev)
+        self.w = torch.zeros(self.n, dtype=dt, device=dev)
+        self.zero = torch.zeros(self.n, dtype=dt, device=dev)
+        self.f = torch.zeros(self.n, dtype=dt, device=dev)
+        self.lam = torch.zeros(self.n, dtype=dt, device=dev)
+        self.r = torch.zeros(self.n, dtype=dt, device=dev)
+        self.pin = torch.zeros(self.n, dtype=dt, device=dev)
+        self.pout = torch.zeros(self.n, dtype=dt, device=dev)
+        self.hb = torch.zeros(2 * self.m + 4, dtype=torch.float64, device=dev)
+        self.y = torch.zeros(self.m, dtype=torch.float64, device=dev)
+        self.parts = torch.zeros(self.lib.glide_dots_parts(self.n) * 32, dtype=torch.float64, device=dev)
+        self._graphs = {}
+        self._cfg = None
+
+    def _s(self):
+        return N.stream_handle()
+
+    def _dots(self, V, k, w, out):
+        N.check(self.lib.glide_dots(self.code, self.n, k, V.data_ptr(), self.n, w.data_ptr(), out.data_ptr(),
+                                    self.parts.data_ptr(), self._s()), "dots")
+
+    def _combine(self, V, k, coef, alpha, out, beta):
+        N.check(self.lib.glide_combine(self.code, self.n, k, V.data_ptr(), self.n, coef.data_ptr(), float(alpha),
+                                       out.data_ptr(), float(beta), self._s()), "combine")
+
+    def _lincomb(self, out, x, a, y=None, b=0.0):
+        N.check(self.lib.glide_lincomb(self.code, out.data_ptr(), x.data_ptr(), float(a),
+                                       None if y is None else y.data_ptr(), float(b), self.n, self._s()), "lincomb")
+
+    def _norm(self, x):
+        self._dots(x, 1, x, self.hb[:1])
+        return math.sqrt(max(float(self.hb[0].item()), 0.0))
+
+    def _apply(self, z, out, exact, active_tol):
+        """out = J_m^T z: glide_vjp gives f - z^T J_m with f = 0."""
+        g = self.ph.grid
+        g.compute_mask(active_tol)
+        a = g.level_args()
+        zu, zv, zH = g._vec_to_fields(z)
+        fu, fv, fH = g._vec_to_fields(self.zero)
+        ou, ov, oH = g._vec_to_fields(out)
+        N.check(self.lib.glide_vjp(C.byref(a), zu.data_ptr(), zv.data_ptr(), zH.data_ptr(), fu.data_ptr(),
+                                   fv.data_ptr(), fH.data_ptr(), ou.data_ptr(), ov.data_ptr(), oH.data_ptr(),
+                                   int(exact), self._s()), "adjoint operator")
+        g.mask.zero_()
+        self._lincomb(out, out, -1.0)
+
+    def _precond_body(self):
+        ph, gc, lib = self.ph, self.gc, self.lib
+        s = self._s()
+        if self.mixed:
+            N.check(lib.glide_convert(N.F32, gc.f_adj.data_ptr(), self.pin.data_ptr(), self.n, 0, s), "convert")
+        else:
+            gc.f_adj.copy_(self.pin)
+        gc.Lambda.zero_()
+        N.check(lib.glide_adjoint_vcycle(ph._native, ph._nlev, 0, C.byref(self._cfg), s), "adjoint_vcycle")
+        if self.mixed:
+            N.check(lib.glide_convert(N.F64, self.pout.data_ptr(), gc.Lambda.data_ptr(), self.n, 1, s), "convert")
+        else:
+            self.pout.copy_(gc.Lambda)
+
+    def _precond(self, key):
+        """pout = one adjoint V-cycle applied to pin (from a CUDA graph)."""
+        if not self.ph.use_graphs:
+            self._precond_body()
+            return
+        entry = self._graphs.get(key)
+        if entry is None:
+            self._precond_body()
+            torch.cuda.synchronize()
+            gr = torch.cuda.CUDAGraph()
+            c0 = self.lib.glide_launch_count()
+            with torch.cuda.graph(gr):
+                self._precond_body()
+            self._graphs[key] = (gr, self.lib.glide_launch_count() - c0)
+            return
+        gr, nodes = entry
+        gr.replay()
+        self.ph.graph_launches += nodes
+
+    def release(self):
+        self._graphs.clear()
+
+    def _linearisation_point(self):
+        """The cycle hierarchy at the step's state: fl32(U) on the FP32
+        hierarchy in the mixed path, the state restricted to every coarse
+        level, gamma = thklim on level 0."""
+        from .kernels import restrict_cell_centered, restrict_hfacet, restrict_vfacet
+        ph = self.ph
+        g = ph.grid
+        g.gamma.fill_(ph.thklim)
+        if self.mixed:
+            N.check(self.lib.glide_convert(N.F32, self.gc.U.data_ptr(), g.U.data_ptr(), self.n, 0, self._s()),
+                    "convert")
+            self.gc.gamma.fill_(ph.thklim)
+        hier = ph.grids32 if self.mixed else ph.grids
+        for par, ch in zip(hier[:-1], hier[1:]):
+            restrict_vfacet(par.u, u_coarse=ch.u)
+            restrict_hfacet(par.v, v_coarse=ch.v)
+            restrict_cell_centered(par.H, f_coarse=ch.H)
+
+    def solve(self, cfg, tol, max_its=300, exact=False, active_tol=0.1):
+        """lam for the current f_adj of the state grid, until |f - J_m^T lam|
+        <= tol |f| or ``max_its`` iterations; lam is left in the state grid's
+        Lambda.  Returns (iterations, relative residual reached)."""
+        ph, m = self.ph, self.m
+        g = ph.grid
+        self._cfg = cfg
+        key = (float(g.dt), int(cfg.exact_adjoint), float(cfg.adj_active_tol))
+        self._linearisation_point()
+        self.f.copy_(g.f_adj)
+        self.lam.zero_()
+        f0 = self._norm(self.f)
+        if not (f0 > 0.0 and math.isfinite(f0)):
+            g.Lambda.zero_()
+            return 0, (0.0 if f0 == 0.0 else float("nan"))
+        self.r.copy_(self.f)
+        rel = 1.0
+        total = 0
+        hb = self.hb
+        while rel > tol and total < max_its:
+            beta = self._norm(self.r)
+            self._lincomb(self.V[0], self.r, 1.0 / beta)
+            Hm = np.zeros((m + 1, m))
+            its, y = 0, None
+            for j in range(m):
+                self.pin.copy_(self.V[j])
+                self._precond(key)
+                self.Z[j].copy_(self.pout)
+                self._apply(self.Z[j], self.w, exact, active_tol)
+                k = j + 1
+                h1, h2, hn = hb[:k], hb[m + 1:m + 1 + k], hb[2 * m + 2:2 * m + 3]
+                self._dots(self.V, k, self.w, h1)
+                self._combine(self.V, k, h1, -1.0, self.w, 1.0)
+                self._dots(self.V, k, self.w, h2)          # second pass (CGS2)
+                self._combine(self.V, k, h2, -1.0, self.w, 1.0)
+                self._dots(self.w, 1, self.w, hn)
+                h = hb.cpu().numpy()
+                Hm[:k, j] = h[:k] + h[m + 1:m + 1 + k]
+                hnorm = math.sqrt(max(h[2 * m + 2], 0.0))
+                Hm[k, j] = hnorm
+                its = k
+                e1 = np.zeros(k + 1)
+                e1[0] = beta
+                y, *_ = np.linalg.lstsq(Hm[:k + 1, :k], e1, rcond=None)
+                est = float(np.linalg.norm(e1 - Hm[:k + 1, :k] @ y)) / f0
+                if not (np.isfinite(est) and np.all(np.isfinite(y))):
+                    its = 0
+                    break
+                if est <= 0.5 * tol or hnorm <= 1e-30 * beta or total + its >= max_its:
+                    break
+                if j + 1 < m:
+                    self._lincomb(self.V[j + 1], self.w, 1.0 / hnorm)
+            if its == 0:
+                rel = float("nan")
+                break
+            total += its
+            self.y[:its].copy_(torch.as_tensor(y, dtype=torch.float64))
+            self._combine(self.Z, its, self.y, 1.0, self.lam, 1.0)
+            # true residual of the restart
+            self._apply(self.lam, self.w, exact, active_tol)
+            self._lincomb(self.r, self.f, 1.0, self.w, -1.0)
+            new = self._norm(self.r) / f0
+            if not math.isfinite(new):
+                rel = new
+                break
+            stalled = new > 0.9 * rel
+            rel = new
+            if stalled:
+                break
+        g.Lambda.copy_(self.lam)
+        g.f_adj.copy_(self.f)
+        return total, rel

@@ -149,7 +149,7 @@ class IcePhysics:
                  finish_step=None, finish_linear=False, finish_patience=3,
                  finish_fas_until=math.inf, finish_fas_patience=10, newton=False, newton_start=1e-3,
                  newton_max_steps=8, newton_rtol=1e-2, newton_krylov=20, newton_min_gain=1.0,
-                 newton_local=0, newton_after=0):
+                 newton_local=0, newton_after=0, adjoint_krylov=30, adjoint_max_its=300):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -188,6 +188,9 @@ class IcePhysics:
         self.newton_local = int(newton_local)
         self.newton_after = int(newton_after)
         self._nk = None
+        self.adjoint_krylov = int(adjoint_krylov)
+        self.adjoint_max_its = int(adjoint_max_its)
+        self._ak = None
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
         self.dtype = _PRECISIONS[precision]
@@ -654,10 +657,14 @@ class IcePhysics:
 
         ``exact=True`` uses the exact transpose at clamped boundary reads in
         the VJP and the gradient (the reference drops some boundary terms).
-        With ``tol`` the adjoint cycles run until |f_adj - J_m^T lam| <=
-        tol |f_adj| (J_m: rows of cells at the thickness limit replaced by the
-        identity, as the adjoint smoother sees them); a cycle that cuts the
-        residual by less than ``stall_factor`` hands over to fine-level
+        With ``tol`` the multiplier is solved until |f_adj - J_m^T lam| <=
+        tol |f_adj| (J_m: rows of the active cells, H <= gamma +
+        ``settings.adj_active_tol``, replaced by the identity, as the adjoint
+        smoother sees them).  With ``adjoint_krylov`` > 0 (the default) by
+        FGMRES preconditioned by one adjoint V-cycle per iteration
+        (``newton.AdjointKrylov``); if that ends above ``tol``, or with
+        ``adjoint_krylov=0``, by adjoint cycles from lam = 0 until a cycle
+        cuts the residual by less than ``stall_factor``, then fine-level
         adjoint sweeps.  A cycle or block of sweeps whose residual is
         non-finite or grows 100x over the best one is undone (the best
         multiplier is kept): a diverging cycle hands over to the sweeps, a
@@ -675,6 +682,19 @@ class IcePhysics:
             g.f_adj_H.copy_(-_as_tensor(dL_dH, g.dtype, self.device))
             g.Lambda.zero_()
             cfg = st.native(self.thklim)
+            if tol is not None and self.adjoint_krylov > 0:
+                from .newton import AdjointKrylov
+                if self._ak is None or self._ak.m != self.adjoint_krylov:
+                    self._ak = AdjointKrylov(self, m=self.adjoint_krylov)
+                its, rel = self._ak.solve(cfg, tol, max_its=self.adjoint_max_its, exact=exact,
+                                          active_tol=st.adj_active_tol)
+                info["krylov_its"] = its
+                if math.isfinite(rel) and rel <= tol:
+                    info["rel_residual"] = rel
+                    self.last_adjoint_info = info
+                    return g.compute_grad_beta(exact_boundary=exact, mask_tol=st.adj_active_tol)
+                info["krylov_rel_residual"] = rel
+                g.Lambda.zero_()
             f0 = None
             n_max = max_vcycles if tol is not None else n_vcycles
             prev = 1.0
@@ -711,7 +731,7 @@ class IcePhysics:
             if tol is not None and rel is not None and rel > tol:
                 done = 0
                 while done < max_finish_sweeps and rel > tol:
-                    g.compute_mask()
+                    g.compute_mask(st.adj_active_tol)
                     g.vanka_sweep_adjoint(self.finish_block, omega=st.adj_omega, exact_boundary=exact)
                     g.mask.zero_()
                     done += self.finish_block
@@ -727,13 +747,13 @@ class IcePhysics:
                 info["finish_sweeps"] = done
             info["rel_residual"] = rel
             self.last_adjoint_info = info
-            return g.compute_grad_beta(exact_boundary=exact)
+            return g.compute_grad_beta(exact_boundary=exact, mask_tol=st.adj_active_tol)
         finally:
             st.exact_adjoint = saved_exact
 
     def _adjoint_rel(self, f0):
         g = self.grid
-        g.compute_mask()
+        g.compute_mask(self.settings.adj_active_tol)
         g.compute_adjoint_residual(self.settings.exact_adjoint)
         g.mask.zero_()
         r = torch.sqrt(torch.sum(g.r_adj.double() ** 2)).item()
@@ -777,6 +797,8 @@ class IcePhysics:
         self._graphs.clear()
         if self._nk is not None:
             self._nk.release()
+        if self._ak is not None:
+            self._ak.release()
 
 
 # ---------------------------------------------------------------------------

@@ -41,6 +41,8 @@ class SolverSettings:
     lin_coarse: int = 20       # linear sweeps on the coarsest level
     lin_omega: float = 0.5     # damping of each linear sweep
     lin_shift: float = 0.0     # diagonal shift of the local factors
+    # adjoint active set: H <= gamma + adj_active_tol (glide/grid.py:332-334 uses 0.1 m)
+    adj_active_tol: float = 0.1
 
     def native(self, thklim) -> N.SolverConfig:
         c = N.SolverConfig()
@@ -56,6 +58,7 @@ class SolverSettings:
         c.pivoted_lu = int(self.pivoted_lu)
         c.lin_pre, c.lin_post, c.lin_coarse = int(self.lin_pre), int(self.lin_post), int(self.lin_coarse)
         c.lin_omega, c.lin_shift = float(self.lin_omega), float(self.lin_shift)
+        c.adj_active_tol = float(self.adj_active_tol)
         return c
 
 

@@ -215,6 +215,9 @@ typedef struct GlideSolverConfig {
     int lin_coarse;         /* linear sweeps on the coarsest level */
     double lin_omega;       /* damping of each linear sweep */
     double lin_shift;       /* diagonal shift of the local factors (0: the local Jacobian) */
+    /* adjoint active set: cells with H <= gamma + adj_active_tol are identity rows
+       of the adjoint system; <= 0 means the reference's 0.1 m (glide/grid.py:332-334) */
+    double adj_active_tol;
 } GlideSolverConfig;
 
 /* One FASCD V-cycle from level k0 (finest=1 sets w=U, chi=gamma-H first). */

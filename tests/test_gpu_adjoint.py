@@ -114,18 +114,19 @@ def test_time_stepped_checkpointed_gradient():
 
 
 def test_adjoint_recovers_from_a_diverging_cycle():
-    """Mixed precision adjoint to a tolerance: a cycle that leaves the
-    multiplier non-finite (planted on the host by overwriting it with NaN
-    after the second cycle) is undone, the fine-level sweeps finish from the
-    best multiplier, and the gradient equals the undisturbed solve's to the
-    tolerance's accuracy."""
+    """Mixed precision adjoint to a tolerance by cycles and sweeps
+    (``adjoint_krylov=0``): a cycle that leaves the multiplier non-finite
+    (planted on the host by overwriting it with NaN after the second cycle)
+    is undone, the fine-level sweeps finish from the best multiplier, and the
+    gradient equals the undisturbed solve's (FGMRES) to the tolerance's
+    accuracy."""
     from glide_b200 import IcePhysics, SolverSettings
     from glide_b200.synthetic import dome_case
     c = dome_case(0, n=64, dx=5000.0, n_levels=3)
 
-    def physics():
+    def physics(krylov=30):
         ph = IcePhysics(64, 64, c.dx, n_levels=3, thklim=c.thklim, precision="mixed",
-                        settings=SolverSettings(shift=0.0, err_threshold=1e-7))
+                        settings=SolverSettings(shift=0.0, err_threshold=1e-7), adjoint_krylov=krylov)
         ph.set_geometry(c.bed, c.thickness)
         ph.set_parameters(B=c.B, beta=c.beta, smb=c.smb)
         ph.forward(c.dt, tol=1e-9, update_geometry=False)
@@ -139,7 +140,7 @@ def test_adjoint_recovers_from_a_diverging_cycle():
     g_ref = ref.adjoint(cu, cv, cH, tol=1e-8).clone()
     assert ref.last_adjoint_info["rel_residual"] <= 1e-8
 
-    ph = physics()
+    ph = physics(krylov=0)   # the cycles-then-sweeps solve
     step = ph._adjoint_dc_step
     calls = []
 

@@ -40,6 +40,21 @@ def test_conv3x3_forward_backward_vs_cpu():
     assert _rel(b.grad, bc.grad) <= 2e-2
 
 
+def test_unet_inference_matches_training_forward_bitwise():
+    """Without autograd the convolutions gather the im2col inside the GEMM;
+    the output is bit-identical to the recorded (im2col-matrix) forward."""
+    from glide_b200.guess import UNet, features
+    torch.manual_seed(1)
+    net = UNet().cuda()
+    H = torch.rand(1, 128, 96, device="cuda") * 1000
+    x = features(H, H * 0.1, torch.full_like(H, 0.1), torch.full_like(H, 35.0))
+    y_train = net(x)
+    assert y_train.requires_grad
+    with torch.no_grad():
+        y_inf = net(x)
+    assert torch.equal(y_train.detach(), y_inf)
+
+
 def test_unet_forward_shapes_and_gradients_flow():
     from glide_b200.guess import UNet, features
     net = UNet().cuda()
