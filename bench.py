@@ -897,10 +897,16 @@ def config_inversion(args, n=512, steps=50, every=10, iters=200, fd_dirs=16, eps
     + a Gaussian random field (20 km correlation, sigma 1) after ``steps``
     implicit steps, with 2 % proportional Gaussian noise; the model runs the
     same steps checkpointed every ``every`` with recomputation (the
-    hand-written VJP behind torch.autograd); central differences on
-    ``fd_dirs`` seeded directions (eps = 1e-6, FP64, steps solved to 1e-10);
-    L-BFGS-B for ``iters`` iterations (mixed precision, steps and adjoints
-    to TOL) with Tikhonov weight 1e-3 on log beta."""
+    hand-written VJP behind torch.autograd).  Misfit: the noise-weighted
+    chi^2 / 2 per observation (sigma = 2 % of |u_obs| + 1 m/a).  Central
+    differences on ``fd_dirs`` seeded directions (eps = 1e-6, FP64, steps
+    and adjoints solved to 1e-10) against two gradients: the reference's
+    adjoint (no grounding-line derivatives in the transposed Jacobian, 0.1 m
+    active-set band) and the exact one (grounding-line derivatives, 1e-6 m
+    band); the first four directions also at 2 eps (smoothness of the step
+    map along them);
+    L-BFGS-B for ``iters`` iterations (mixed precision, steps and adjoints to
+    TOL) with Tikhonov weight 1e-3 on log beta."""
     import numpy as np
     import torch
     from glide_b200 import IcePhysics
@@ -913,12 +919,12 @@ def config_inversion(args, n=512, steps=50, every=10, iters=200, fd_dirs=16, eps
     logb_ref = float(np.log(beta_head(1e3)))
     logb_true = logb_ref + _grf(rng, n, n, c.dx, 20e3)
 
-    def physics(precision):
+    def physics(precision, **extra):
         # the FP64 model of the finite differences is solved to 1e-10: sweeps-only finish
         kw = dict(settings=fast_settings(),
                   **(FAST_KW if precision == "mixed" else {k: v for k, v in FP64_FAST_KW.items()
                                                            if not k.startswith("newton")}))
-        ph = IcePhysics(n, n, c.dx, n_levels=c.n_levels, thklim=c.thklim, precision=precision, **kw)
+        ph = IcePhysics(n, n, c.dx, n_levels=c.n_levels, thklim=c.thklim, precision=precision, **kw, **extra)
         ph.set_geometry(c.bed, c.thickness)
         ph.set_parameters(B=c.B, beta=np.exp(logb_true), smb=c.smb)
         return ph
@@ -934,22 +940,40 @@ def config_inversion(args, n=512, steps=50, every=10, iters=200, fd_dirs=16, eps
         v_obs = v * (1.0 + 0.02 * torch.randn(v.shape, generator=torch.Generator().manual_seed(6),
                                               dtype=v.dtype).to(v.device))
     t_obs = time.time() - t0
+    sig_u = 0.02 * u.abs() + 1.0
+    sig_v = 0.02 * v.abs() + 1.0
+    wkw = dict(sigma_u=sig_u, sigma_v=sig_v, normalize=True)
     x0 = np.full(n * n, logb_ref)
     out = {"grid": f"{n}x{n}, dx={c.dx:g} m, {c.n_levels} levels, dt={c.dt:g} a", "steps": steps,
            "checkpoint_every": every, "observations_s": t_obs}
     # gradient check in FP64
     ph64 = physics("fp64")
     obj64 = TimeSteppedObjective(ph64, H0, u_obs, v_obs, c.dt, steps, every, reg_weight=1e-3, tol=1e-10,
-                                 adj_tol=1e-10)
+                                 adj_tol=1e-10, **wkw)
     t0 = time.time()
-    errs, pairs = finite_difference_check(obj64, x0, n_directions=fd_dirs, eps=eps)
-    out["fd_check"] = {"directions": fd_dirs, "eps": eps, "rel_err": errs, "max_rel_err": max(errs),
-                       "median_rel_err": float(np.median(errs)), "s": time.time() - t0,
-                       "max_step_rel_residual": obj64.max_step_rel, "tol": 1e-10}
+    _, g_ref = obj64(x0)
+    ph64x = physics("fp64", gl_derivatives=True)
+    ph64x.settings.adj_active_tol = 1e-6
+    obj64x = TimeSteppedObjective(ph64x, H0, u_obs, v_obs, c.dt, steps, every, reg_weight=1e-3, tol=1e-10,
+                                  adj_tol=1e-10, **wkw)
+    _, g_exact = obj64x(x0)
+    del obj64x, ph64x
+    (e_ref, e_exact), pairs, smooth = finite_difference_check(obj64, x0, n_directions=fd_dirs, eps=eps,
+                                                              grads=[g_ref, g_exact], smooth_dirs=min(4, fd_dirs))
+
+    def stats(e):
+        return {"rel_err": e, "max": max(e), "median": float(np.median(e))}
+    out["fd_check"] = {"directions": fd_dirs, "eps": eps, "s": time.time() - t0,
+                       "reference_adjoint": stats(e_ref), "exact_adjoint": stats(e_exact),
+                       "fd_eps_vs_2eps_rel": smooth, "pairs_fd_ref_exact": pairs,
+                       "max_step_rel_residual": obj64.max_step_rel, "tol": 1e-10,
+                       "note": "reference_adjoint: J^T without grounding-line derivatives, active set H <= thklim "
+                               "+ 0.1 m; exact_adjoint: with them, active set H <= thklim + 1e-6 m"}
     del obj64, ph64
     torch.cuda.empty_cache()
     # L-BFGS in mixed precision
-    obj = TimeSteppedObjective(ph, H0, u_obs, v_obs, c.dt, steps, every, reg_weight=1e-3, tol=TOL, adj_tol=TOL)
+    obj = TimeSteppedObjective(ph, H0, u_obs, v_obs, c.dt, steps, every, reg_weight=1e-3, tol=TOL, adj_tol=TOL,
+                               **wkw)
     t0 = time.time()
     x, rec = invert_time_stepped(obj, x0, maxiter=iters)
     t_inv = time.time() - t0

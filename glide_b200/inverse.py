@@ -182,12 +182,18 @@ class TimeSteppedObjective:
     passes it."""
 
     def __init__(self, physics, H0, u_obs, v_obs, dt, n_steps, checkpoint_every=10, reg_weight=1e-3, tol=1e-8,
-                 adj_tol=1e-8, max_vcycles=60):
+                 adj_tol=1e-8, max_vcycles=60, sigma_u=None, sigma_v=None, normalize=False):
         g = physics.grid
         self.ph, self.dt, self.n, self.every = physics, float(dt), int(n_steps), int(checkpoint_every)
         self.H0 = torch.as_tensor(H0, dtype=g.dtype, device=g.device)
         self.u_obs = torch.as_tensor(u_obs, dtype=g.dtype, device=g.device)
         self.v_obs = torch.as_tensor(v_obs, dtype=g.dtype, device=g.device)
+        # misfit weights 1/sigma^2 (1 without sigma), divided by the number of observations with ``normalize``
+        scale = 1.0 / (self.u_obs.numel() + self.v_obs.numel()) if normalize else 1.0
+        self.w_u = scale / torch.as_tensor(sigma_u, dtype=g.dtype, device=g.device) ** 2 if sigma_u is not None \
+            else torch.full_like(self.u_obs, scale)
+        self.w_v = scale / torch.as_tensor(sigma_v, dtype=g.dtype, device=g.device) ** 2 if sigma_v is not None \
+            else torch.full_like(self.v_obs, scale)
         self.reg_weight, self.tol, self.adj_tol, self.max_vcycles = float(reg_weight), tol, adj_tol, max_vcycles
         self.shape = (g.ny, g.nx)
         self.evaluations = 0
@@ -201,7 +207,7 @@ class TimeSteppedObjective:
         self.ph.solve_log = []
         u, v, _ = time_stepped(beta, self.H0, self.ph, self.dt, self.n, self.every, self.tol, self.adj_tol,
                                self.max_vcycles)
-        J = 0.5 * ((u - self.u_obs) ** 2).sum() + 0.5 * ((v - self.v_obs) ** 2).sum()
+        J = self._misfit(u, v)
         J.backward()
         t, gt = tikhonov(logb.detach())
         grad = beta.grad * beta.detach() + self.reg_weight * gt
@@ -214,6 +220,9 @@ class TimeSteppedObjective:
                      "adjoint_rel_residual": getattr(self.ph, "last_adjoint_info", {}).get("rel_residual")}
         self.max_step_rel = max(self.max_step_rel, max(rels) if rels else 0.0)
         return total, grad
+
+    def _misfit(self, u, v):
+        return 0.5 * (self.w_u * (u - self.u_obs) ** 2).sum() + 0.5 * (self.w_v * (v - self.v_obs) ** 2).sum()
 
     def _logb(self, x):
         g = self.ph.grid
@@ -231,7 +240,7 @@ class TimeSteppedObjective:
         with torch.no_grad():
             u, v, _ = time_stepped(torch.exp(logb), self.H0, self.ph, self.dt, self.n, self.every, self.tol,
                                    self.adj_tol, self.max_vcycles)
-            J = 0.5 * ((u - self.u_obs) ** 2).sum() + 0.5 * ((v - self.v_obs) ** 2).sum()
+            J = self._misfit(u, v)
         rels = [r for r in self.ph.solve_log if r is not None]
         self.ph.solve_log = None
         self.max_step_rel = max(self.max_step_rel, max(rels) if rels else 0.0)
@@ -239,33 +248,55 @@ class TimeSteppedObjective:
         return float(J) + self.reg_weight * float(t)
 
 
-def finite_difference_check(objective, x, n_directions=16, eps=1e-6, seed=0):
+def finite_difference_check(objective, x, n_directions=16, eps=1e-6, seed=0, grads=None, smooth_dirs=0):
     """Central differences (L(x + eps d) - L(x - eps d)) / (2 eps) of a
     ``TimeSteppedObjective`` along ``n_directions`` seeded unit-variance
-    directions d, against grad . d from its adjoint.  Returns the relative
-    differences |fd - ad| / |fd| and the pairs (fd, ad)."""
+    directions d, against grad . d from its adjoint (or, with ``grads``, from
+    each of several precomputed gradients).  Returns the relative differences
+    |fd - ad| / |fd| (a list per gradient when ``grads`` is given), the pairs
+    (fd, ad) and, for the first ``smooth_dirs`` directions, the relative
+    difference of the central differences at eps and 2 eps: a large one means
+    the step map is not smooth along d at this scale (a cell changes solution
+    branch), so no gradient can match that direction's differences."""
     rng = np.random.default_rng(seed)
-    _, grad = objective(x)
-    errs, pairs = [], []
-    for _ in range(n_directions):
+    if grads is None:
+        _, grad = objective(x)
+        glist = [grad]
+    else:
+        glist = list(grads)
+    errs = [[] for _ in glist]
+    pairs, smooth = [], []
+    for k in range(n_directions):
         d = rng.standard_normal(x.size)
         fp = objective.value(x + eps * d)
         fm = objective.value(x - eps * d)
         fd = (fp - fm) / (2.0 * eps)
-        ad = float(grad @ d)
-        errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
-        pairs.append((fd, ad))
-    return errs, pairs
+        ads = [float(g @ d) for g in glist]
+        for e, ad in zip(errs, ads):
+            e.append(abs(fd - ad) / max(abs(fd), 1e-300))
+        pairs.append((fd, *ads))
+        if k < smooth_dirs:
+            fd2 = (objective.value(x + 2 * eps * d) - objective.value(x - 2 * eps * d)) / (4.0 * eps)
+            smooth.append(abs(fd2 - fd) / max(abs(fd), 1e-300))
+    return (errs[0] if grads is None else errs), pairs, smooth
 
 
 def invert_time_stepped(objective, x0, *, maxiter=200, bounds=(-6.0, 5.0), m=15, factr=1e7, callback=None):
     """L-BFGS-B over log beta of a ``TimeSteppedObjective`` (``maxiter``
-    iterations at most).  Returns the optimum and a record."""
+    iterations at most).  Returns the optimum and a record (with the misfit
+    and objective after every iteration)."""
     from scipy.optimize import fmin_l_bfgs_b
     f0, _ = objective(x0)
     first = dict(objective.last)
+    history = []
+
+    def cb(xk):
+        history.append((objective.last["misfit"], objective.last["total"]))
+        if callback is not None:
+            callback(xk)
     x, f, info = fmin_l_bfgs_b(objective, x0, bounds=[bounds] * x0.size, m=m, factr=factr, maxiter=maxiter,
-                               callback=callback)
+                               callback=cb)
     return x, {"initial": first, "final": dict(objective.last), "final_total": float(f),
                "iterations": int(info["nit"]), "evaluations": objective.evaluations,
-               "warnflag": int(info["warnflag"])}
+               "warnflag": int(info["warnflag"]), "task": str(info.get("task", "")),
+               "misfit_total_per_iteration": history}
