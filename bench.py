@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--kernels-compare", action="store_true",
                     help="per-call times of the hot kernels at 1024^2 and 4096^2 (with --impl reference: the "
                          "reference's own kernels on the same state)")
+    ap.add_argument("--guess-kernels", action="store_true",
+                    help="tensor-core convolutions of the learned guess at 1024^2: per layer TFLOP/s and the "
+                         "whole inference time")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying CUDA graphs (for profiler runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -1204,6 +1207,60 @@ def kernel_compare_ours(args):
                       "case": "marine (floating shelves), seeded random velocities"}), flush=True)
 
 
+def guess_kernel_table(args, n=1024, reps=20):
+    """Every 3x3 convolution of the guess network at its shape for an n x n
+    input (implicit-GEMM tcgen05 kernel, BF16 in, FP32 accumulate, bias +
+    ReLU, BF16 out), CUDA events over ``reps`` launches after 3 warm-up
+    launches; and one whole inference on a bench geometry.  TFLOP/s against
+    the measured cuBLAS BF16 peak (burst)."""
+    import torch
+    from glide_b200 import guess as G
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    peak = float(peaks["bf16_tflops"])
+    model = G.load_default_model()
+    net = model.net
+    side = []
+    hw = n
+    for lv in range(net.levels):
+        side += [hw, hw]
+        if lv < net.levels - 1:
+            hw //= 2
+    for lv in range(net.levels - 2, -1, -1):
+        hw *= 2
+        side += [hw, hw]
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+    rows = []
+    g = torch.Generator(device="cuda").manual_seed(0)
+    with torch.no_grad():
+        for (cin, cout), h in zip(net.plan, side):
+            x = torch.randn(1, h, h, cin, generator=g, device="cuda").to(torch.bfloat16)
+            W = (torch.randn(cout, 9 * cin, generator=g, device="cuda") * 0.05).to(torch.bfloat16)
+            bias = torch.zeros(cout, device="cuda")
+            y = torch.empty((h * h, cout), dtype=torch.bfloat16, device="cuda")
+            ms = timed(lambda: G.conv3x3(x, W, y, bias=bias, relu=True, out_mode=1))
+            fl = 2.0 * h * h * 9 * cin * cout
+            rows.append({"hw": h, "cin": cin, "cout": cout, "us": round(ms * 1e3, 1),
+                         "tflops": round(fl / ms / 1e9, 1), "frac_of_measured_bf16": round(fl / ms / 1e9 / peak, 4)})
+        case = make_cases(n, [5])[0]
+        dev = {k: torch.as_tensor(v, device="cuda") for k, v in (("H", case.thickness), ("bed", case.bed),
+                                                                 ("beta", case.beta), ("B", case.B))}
+        ms_inf = timed(lambda: model.predict(dev["H"], dev["bed"], dev["beta"], dev["B"]))
+    print(json.dumps({"guess_kernels": rows, "inference_ms": round(ms_inf, 3),
+                      "inference_gflop": round(net.flops(n, n) / 1e9, 1), "bf16_peak_tflops": peak,
+                      "peak_source": "measured (cuBLAS bf16 8192^3, burst)"}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference" and args.kernels_compare:
@@ -1214,6 +1271,8 @@ def main():
         run_reference(args)
     elif args.kernels:
         kernel_table(args)
+    elif args.guess_kernels:
+        guess_kernel_table(args)
     elif args.configs:
         run_configs(args)
     else:

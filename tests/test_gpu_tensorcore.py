@@ -117,3 +117,24 @@ def test_implicit_conv3x3_equals_im2col_gemm(C_in, C_out, out_mode):
     conv3x3(x, Wb, b, bias=bias, relu=True, out_mode=out_mode)
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("N", [24, 64, 96, 200])
+def test_pipelined_and_single_stage_gemm_agree(N):
+    """Aligned operands run the cp.async-pipelined kernel (N tile 32, 64 or
+    128 after the output width); an A with a row pitch that is not a multiple
+    of 8 elements runs the single-stage kernel.  Both accumulate the same BF16
+    products in FP32 chunk by chunk: results agree to FP32 rounding, and both
+    match the FP32 product."""
+    torch.manual_seed(N)
+    M, K = 300, 136
+    A = torch.randn(M, K, device="cuda").bfloat16()
+    B = torch.randn(N, K, device="cuda").bfloat16()
+    A_pad = torch.zeros(M, K + 4, device="cuda").bfloat16()
+    A_pad[:, :K] = A
+    bias = torch.randn(N, device="cuda")
+    p = gemm(A, B, bias=bias, relu=True, out_mode=0)
+    s = gemm(A_pad[:, :K], B, bias=bias, relu=True, out_mode=0)
+    ref = torch.relu(A.float() @ B.float().T + bias)
+    assert (p - s).abs().max().item() <= 1e-5 * (ref.abs().max().item() + 1)
+    assert (p - ref).abs().max().item() <= 1e-3 * (ref.abs().max().item() + 1)
