@@ -281,22 +281,35 @@ def finite_difference_check(objective, x, n_directions=16, eps=1e-6, seed=0, gra
     return (errs[0] if grads is None else errs), pairs, smooth
 
 
-def invert_time_stepped(objective, x0, *, maxiter=200, bounds=(-6.0, 5.0), m=15, factr=1e7, callback=None):
+def invert_time_stepped(objective, x0, *, maxiter=200, bounds=(-6.0, 5.0), m=15, factr=1e7, callback=None,
+                        max_seconds=None):
     """L-BFGS-B over log beta of a ``TimeSteppedObjective`` (``maxiter``
-    iterations at most).  Returns the optimum and a record (with the misfit
-    and objective after every iteration)."""
-    from scipy.optimize import fmin_l_bfgs_b
+    iterations at most; with ``max_seconds``, no new iteration starts after
+    that wall time).  Returns the last accepted iterate and a record (with the
+    misfit and objective after every iteration)."""
+    import time
+
+    from scipy.optimize import minimize
+    t0 = time.time()
     f0, _ = objective(x0)
     first = dict(objective.last)
     history = []
+    best = {"x": np.array(x0, dtype=np.float64), "f": f0}
+    stopped = {"time": False}
 
     def cb(xk):
         history.append((objective.last["misfit"], objective.last["total"]))
+        best["x"] = np.array(xk, dtype=np.float64)
+        best["f"] = objective.last["total"]
         if callback is not None:
             callback(xk)
-    x, f, info = fmin_l_bfgs_b(objective, x0, bounds=[bounds] * x0.size, m=m, factr=factr, maxiter=maxiter,
-                               callback=cb)
-    return x, {"initial": first, "final": dict(objective.last), "final_total": float(f),
-               "iterations": int(info["nit"]), "evaluations": objective.evaluations,
-               "warnflag": int(info["warnflag"]), "task": str(info.get("task", "")),
+        if max_seconds is not None and time.time() - t0 > max_seconds:
+            stopped["time"] = True
+            raise StopIteration
+    res = minimize(objective, x0, jac=True, method="L-BFGS-B", bounds=[bounds] * x0.size, callback=cb,
+                   options={"maxiter": maxiter, "maxcor": m, "ftol": factr * np.finfo(float).eps})
+    x = res.x if not stopped["time"] else best["x"]
+    return x, {"initial": first, "final": dict(objective.last), "final_total": float(best["f"]),
+               "iterations": len(history), "evaluations": objective.evaluations,
+               "stopped_on_time": stopped["time"], "message": str(res.message),
                "misfit_total_per_iteration": history}

@@ -271,8 +271,11 @@ class AdjointKrylov:
     graph; on the FP32 hierarchy in the mixed path, its input and output
     converted).  The Krylov vectors, the operator (``glide_vjp``) and the
     residual it reports are in the state's precision, so the mixed path's
-    multiplier solves the FP64 system.  No counterpart in the reference, which
-    runs two adjoint V-cycles (glide/physics.py:211-242)."""
+    multiplier solves the FP64 system.  With the physics'
+    ``adjoint_exact_jacobian`` the operator includes the grounding-line
+    derivatives (the transpose of the exact Jacobian) while the
+    preconditioner keeps the solver's own Jacobian.  No counterpart in the
+    reference, which runs two adjoint V-cycles (glide/physics.py:211-242)."""
 
     def __init__(self, physics, m=30):
         self.ph = physics
@@ -323,6 +326,8 @@ class AdjointKrylov:
         g = self.ph.grid
         g.compute_mask(active_tol)
         a = g.level_args()
+        if self.ph.adjoint_exact_jacobian:
+            a.params.gl_derivatives = 1
         zu, zv, zH = g._vec_to_fields(z)
         fu, fv, fH = g._vec_to_fields(self.zero)
         ou, ov, oH = g._vec_to_fields(out)

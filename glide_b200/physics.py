@@ -149,7 +149,8 @@ class IcePhysics:
                  finish_step=None, finish_linear=False, finish_patience=3,
                  finish_fas_until=math.inf, finish_fas_patience=10, newton=False, newton_start=1e-3,
                  newton_max_steps=8, newton_rtol=1e-2, newton_krylov=20, newton_min_gain=1.0,
-                 newton_local=0, newton_after=0, adjoint_krylov=30, adjoint_max_its=300):
+                 newton_local=0, newton_after=0, newton_tries=6, adjoint_krylov=30, adjoint_max_its=300,
+                 adjoint_exact_jacobian=False, branch_hops=2):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         if not torch.cuda.is_available():
@@ -187,9 +188,16 @@ class IcePhysics:
         self.newton_min_gain = float(newton_min_gain)
         self.newton_local = int(newton_local)
         self.newton_after = int(newton_after)
+        self.newton_tries = int(newton_tries)
         self._nk = None
         self.adjoint_krylov = int(adjoint_krylov)
         self.adjoint_max_its = int(adjoint_max_its)
+        if adjoint_exact_jacobian and self.adjoint_krylov <= 0:
+            raise ValueError("adjoint_exact_jacobian needs the Krylov adjoint (adjoint_krylov > 0)")
+        # the tolerance adjoint's operator with the grounding-line derivatives (the forward solve and the
+        # adjoint cycles keep gl_derivatives)
+        self.adjoint_exact_jacobian = bool(adjoint_exact_jacobian)
+        self.branch_hops = int(branch_hops)
         self._ak = None
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.kernels = N.load()
@@ -467,8 +475,14 @@ class IcePhysics:
         near 1e-4, 2e-4 and 8 blocks suit both fresh and warm-started steps.
         Ten blocks without
         progress restore the best state and continue in FP64 with the
-        reference's damped local Newton and no extrapolation; a second
-        stagnation ends the finish.
+        reference's damped local Newton and no extrapolation.  Divergence or
+        stagnation in that safe mode restores the best state again, halves the
+        sweeps' omega and lets the Newton-Krylov finish try again (up to
+        ``newton_tries`` attempts in all).  When omega would fall below 1/16
+        of the setting, the cell with the largest residual is moved to the
+        other root of its mass balance (``_branch_hop``, at most
+        ``branch_hops`` times) and the finish starts over from there; the
+        best state over all attempts is kept.  It ends at ``max_sweeps``.
         """
         g = self.grid
         st = self.settings
@@ -491,9 +505,41 @@ class IcePhysics:
         fas_until = self.finish_fas_until
         nk_last = math.inf   # |r|/|r0| at the last Newton-Krylov attempt
         nk_tries = 0
+        damp = 1.0           # omega factor of the safe mode's FP64 sweeps
+        hops = 0
+        hop_keep, hop_rel = None, math.inf   # best state before the last branch hop
+
+        def hop():
+            """Move the worst cell to its other mass-balance root; restart the finish state."""
+            nonlocal hops, hop_keep, hop_rel, rel, best, since_best, nk_last, nk_tries, damp, local, use32, m
+            nonlocal prev, form32
+            if hops >= self.branch_hops:
+                return False
+            if best < hop_rel:
+                if hop_keep is None:
+                    hop_keep = torch.empty_like(g.U)
+                hop_keep.copy_(good)
+                hop_rel = best
+            g.U.copy_(good)
+            if not self._branch_hop():
+                return False
+            hops += 1
+            info["branch_hops"] = hops
+            rel = self.residual_norm() / r0 if r0 > 0 else 0.0
+            best = prev = rel
+            good.copy_(g.U)
+            since_best, nk_last, nk_tries, damp = 0, math.inf, 0, 1.0
+            local = self._finish_local()
+            use32 = self.grid32 is not None and self.finish_fp32
+            form32 = "linear" if self.finish_linear is True else "fas"
+            m = self.finish_anderson
+            if aa is not None:
+                aa.reset()
+            hist.append(rel)
+            return True
         while done < max_sweeps and rel > tol:
-            if (self.newton and rel <= self.newton_start and rel < 0.5 * nk_last and nk_tries < 3 and
-                    done >= self.newton_after):
+            if (self.newton and rel <= self.newton_start and rel < 0.5 * nk_last and
+                    nk_tries < self.newton_tries and done >= self.newton_after):
                 # Newton-Krylov from here; a failed attempt falls back to the blocks below, and a
                 # new attempt follows once they have halved the residual
                 nk_tries += 1
@@ -518,7 +564,7 @@ class IcePhysics:
             elif use32:
                 self._fp32_sweeps(self.finish_block, local)
             else:
-                g.vanka_sweep(self.finish_block, omega=st.omega, shift=st.shift, **local)
+                g.vanka_sweep(self.finish_block, omega=st.omega * damp, shift=st.shift, **local)
             done += self.finish_block
             if m > 0:
                 # an extrapolation that raises |r| is kept on purpose: measured, it shortens the finish
@@ -535,7 +581,20 @@ class IcePhysics:
                 rel = best
                 safe = dict(n_inner=REFERENCE.n_newton, step=REFERENCE.newton_step)
                 if local == safe and m == 0:
-                    break
+                    # diverged in the safe mode too: on in FP64, then with more damping; Newton-Krylov
+                    # may try again from the best state
+                    if use32:
+                        use32 = False
+                    else:
+                        damp *= 0.5
+                        if damp < 1.0 / 16:
+                            if hop():
+                                continue
+                            break
+                        info["finish_damp"] = damp
+                    nk_last = math.inf
+                    since_best = 0
+                    continue
                 local, m = safe, 0
                 info["finish_safe"] = True
                 continue
@@ -547,12 +606,19 @@ class IcePhysics:
             since_best += 1
             if since_best > 10:
                 # no progress over 10 blocks: back to the best state and on in FP64 with the reference's
-                # damped local Newton and no extrapolation; a second stagnation ends the finish (a late
-                # guess fallback may follow)
+                # damped local Newton and no extrapolation; a stagnation in that mode halves omega (and
+                # lets Newton-Krylov try again) until omega would fall below 1/16 (then a late guess
+                # fallback may follow)
                 safe = dict(n_inner=REFERENCE.n_newton, step=REFERENCE.newton_step)
                 if local == safe and not use32 and m == 0:
-                    info["finish_stagnated"] = True
-                    break
+                    damp *= 0.5
+                    if damp < 1.0 / 16:
+                        if hop():
+                            continue
+                        info["finish_stagnated"] = True
+                        break
+                    info["finish_damp"] = damp
+                    nk_last = math.inf
                 g.U.copy_(good)
                 rel = best
                 local, use32, m = safe, False, 0
@@ -579,8 +645,50 @@ class IcePhysics:
                 if aa is not None:
                     aa.reset()
             prev = rel
+        if hop_keep is not None and not rel <= hop_rel:
+            g.U.copy_(hop_keep)   # the hops did not pay: back to the best state before them
+            rel = hop_rel
         info["finish_sweeps"] = done
         return rel
+
+    def _branch_hop(self):
+        """Move the cell with the largest residual to the other root of its
+        own mass balance, velocities and the neighbours' fluxes held fixed.
+
+        With the net outflow D of the cell at the current state,
+        r_H(H) = H/dt + c (1 - g(H)) H + D - f_H (glide/cuda/flux.cu:187-211)
+        has a grounded root H = (f_H - D) dt and a floating root
+        H = (f_H - D) / (1/dt + c) when the flotation thickness -bed/0.917
+        lies between them.  A finish that stalls at a handful of cells at the
+        grounding line sits where the branch it follows ends (the two roots
+        merge); the step's solution there is on the other branch.  Returns
+        False when the cell has no other root."""
+        g = self.grid
+        g.gamma.fill_(self.thklim)
+        g.compute_residual()
+        Hm = g.H - g.gamma
+        rH = g.r_H
+        fb = (Hm + rH - torch.sqrt(Hm * Hm + rH * rH)).abs().flatten()
+        k = int(torch.argmax(fb).item())
+        H = float(g.H.flatten()[k])
+        bed = float(g.bed.flatten()[k])
+        fH = float(g.f_H.flatten()[k])
+        r = float(rH.flatten()[k])
+        dt, c = float(g.dt), self.calving_rate
+        z = max(min(self.gl_sigmoid_c * (bed + RHO_ICE / 1000.0 * H), 20.0), -20.0)
+        gnd = 1.0 / (1.0 + math.exp(-z))
+        S = fH - (r - H / dt - c * (1.0 - gnd) * H + fH)   # f_H - D
+        flot = -bed / (RHO_ICE / 1000.0)
+        if gnd > 0.5:
+            H_new = S / (1.0 / dt + c)
+            ok = H_new < flot
+        else:
+            H_new = S * dt
+            ok = H_new > flot
+        if not (ok and math.isfinite(H_new) and H_new > self.thklim):
+            return False
+        g.H.view(-1)[k] = H_new
+        return True
 
     def _newton_krylov(self):
         from .newton import NewtonKrylov
@@ -694,6 +802,11 @@ class IcePhysics:
                     self.last_adjoint_info = info
                     return g.compute_grad_beta(exact_boundary=exact, mask_tol=st.adj_active_tol)
                 info["krylov_rel_residual"] = rel
+                if self.adjoint_exact_jacobian:
+                    # the cycles below solve the solver's own adjoint, not the exact one
+                    info["rel_residual"] = rel
+                    self.last_adjoint_info = info
+                    return g.compute_grad_beta(exact_boundary=exact, mask_tol=st.adj_active_tol)
                 g.Lambda.zero_()
             f0 = None
             n_max = max_vcycles if tol is not None else n_vcycles
