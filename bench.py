@@ -794,11 +794,11 @@ def cpu_baseline(case, infos, workers=None):
                                         f"scaled to {case.ny} rows ({t1:.1f} s per sweep) and to a step as above"}}
 
 
-# mean counts of the plain FP64 arm on this workload (GPU run of the default
-# bench: the 8 timed fresh geometries, seeds 3-10)
 TOL_TIGHT = 1e-8   # tolerance of the reference solutions of the accuracy check
-REF_VCYCLES_PER_STEP = 3.125
-REF_FINISH_SWEEPS_PER_STEP = 937.5
+# mean counts of the plain FP64 arm on this workload (GPU run of the default
+# bench: the 20 timed fresh geometries, seeds 5-24)
+REF_VCYCLES_PER_STEP = 3.15
+REF_FINISH_SWEEPS_PER_STEP = 991.0
 
 
 def run_reference(args):
