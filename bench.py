@@ -256,7 +256,9 @@ class Runner:
     def continue_step(self, dev, U, tol, max_finish_sweeps=MAX_FINISH):
         """Continue a solved step of the geometry ``dev`` from the state ``U``
         (a host or device FP64 vector) to ``tol``, relative to the residual of
-        the step's starting state (so the answer stays on U's solution branch)."""
+        the step's starting state, with the finishing sweeps alone (no FAS
+        cycle, which can carry a converged state onto another solution
+        branch), so the answer stays on U's branch."""
         ph = self.ph
         ph.set_geometry(dev["bed"], dev["H"])
         ph.set_parameters(B=dev["B"], beta=dev["beta"], smb=dev["smb"])
@@ -266,8 +268,7 @@ class Runner:
         g.f_H.copy_(g.H_prev / DT + g.smb)
         r0 = ph.residual_norm()
         g.U.copy_(U.to(device=g.U.device, dtype=g.U.dtype))
-        ph.forward(DT, tol=tol, max_vcycles=self.max_vcycles, max_finish_sweeps=max_finish_sweeps, r0=r0,
-                   update_geometry=False)
+        ph.forward(DT, tol=tol, max_vcycles=0, max_finish_sweeps=max_finish_sweeps, r0=r0, update_geometry=False)
         return dict(ph.last_info)
 
 
@@ -601,6 +602,10 @@ def run_ours(args):
            "dropped_seeds": [timed_seeds[k] for k in range(args.steps) if k not in kept],
            "note": "largest relative 2-norm difference per field over the timed steps whose reference reached "
                    f"{TOL_TIGHT:g}; dropped_seeds lists those that did not"}
+    if kept:
+        per = [solution_error([sols["fast"][k]], [sol_tight[k]], n)["u"] for k in kept]
+        err["fast_u_per_seed"] = {str(timed_seeds[k]): e for k, e in zip(kept, per)}
+        err["continuation_changed_branch"] = [timed_seeds[k] for k, e in zip(kept, per) if e > 1e-3]
     if sols["plain_fp64_fas"]:
         err["fast_vs_plain_fp64"] = solution_error(sols["fast"], sols["plain_fp64_fas"], n)
         if sols["learned_guess"]:

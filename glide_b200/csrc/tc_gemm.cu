@@ -12,8 +12,9 @@
 // four tcgen05.mma (M=128, K=16) per 64-wide K chunk into a TMEM accumulator
 // and commits them to an mbarrier; the epilogue reads TMEM with tcgen05.ld
 // (each warp its 32-lane subpartition).  Two kernels:
-//  * tc_gemm_pipe_kernel (aligned operands, every convolution): a 4-stage
-//    ring filled by cp.async, N tile 32/64/128 after the output width;
+//  * tc_gemm_pipe_kernel (aligned operands, every convolution): a 2-stage
+//    (short K) or 4-stage ring filled by cp.async, N tile 32/64/128 after
+//    the output width;
 //  * tc_gemm_kernel (any pitch or K): one 128 x 64 tile staged through
 //    registers per chunk, every thread waiting for its MMAs before the next.
 //
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(GTHREADS) tc_gemm_kernel(const __nv_bfloat16* 
 // once for 128 outputs.  The epilogue stores 8 BF16 outputs per 16-byte
 // store where the row allows it.
 // --------------------------------------------------------------------------
-constexpr int PSTAGES = 4;
+constexpr int PSTAGES_MAX = 4;
 
 __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* src, uint32_t src_bytes) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(src), "r"(src_bytes)
@@ -269,7 +270,7 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <bool CONV, int BN>
+template <bool CONV, int BN, int PSTAGES>
 __global__ void __launch_bounds__(GTHREADS) tc_gemm_pipe_kernel(const __nv_bfloat16* __restrict__ A, int lda,
                                                                 const __nv_bfloat16* __restrict__ B, int ldb,
                                                                 void* C, int ldc, int M, int N, int K,
@@ -278,7 +279,7 @@ __global__ void __launch_bounds__(GTHREADS) tc_gemm_pipe_kernel(const __nv_bfloa
     constexpr int A_BYTES = GM * GK * 2, B_BYTES = BN * GK * 2, STAGE = A_BYTES + B_BYTES;
     constexpr int AROWS = GM / 16, BROWS = BN / 16;   // rows per thread and chunk
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar[PSTAGES];
+    __shared__ __align__(8) uint64_t mbar[PSTAGES_MAX];
     __shared__ uint32_t tmem_slot;
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -457,7 +458,7 @@ __global__ void __launch_bounds__(GTHREADS) tc_gemm_pipe_kernel(const __nv_bfloa
     }
 }
 
-template <bool CONV, int BN>
+template <bool CONV, int BN, int PSTAGES>
 int launch_pipe(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, void* C, int ldc, int M, int N,
                 int K, const float* bias, int relu, int out_mode, int* err, ConvShape cs, cudaStream_t s) {
     constexpr int SMEM = PSTAGES * (GM * GK * 2 + BN * GK * 2) + 1024;
@@ -466,23 +467,35 @@ int launch_pipe(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return GLIDE_E_SHAPE;
     if (!configured[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(tc_gemm_pipe_kernel<CONV, BN>,
+        const cudaError_t e = cudaFuncSetAttribute(tc_gemm_pipe_kernel<CONV, BN, PSTAGES>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
         if (e != cudaSuccess) return int(e);
         configured[dev] = 1;
     }
     dim3 grid((M + GM - 1) / GM, (N + BN - 1) / BN);
-    count_launch(), tc_gemm_pipe_kernel<CONV, BN><<<grid, GTHREADS, SMEM, s>>>(A, lda, B, ldb, C, ldc, M, N, K, bias,
-                                                                              relu, out_mode, err, cs);
+    count_launch(), tc_gemm_pipe_kernel<CONV, BN, PSTAGES><<<grid, GTHREADS, SMEM, s>>>(
+        A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs);
     return int(cudaGetLastError());
+}
+
+// Short K (a few chunks, the convolutions of the guess network) runs a
+// 2-stage ring: half the shared memory, so 2-3x the CTAs per SM hide each
+// CTA's fixed latencies (ncu at 1024^2, C = 32, 4 stages: 2 CTAs and 7.7
+// warps per SM, tensor pipe 3 % active); long K keeps 4 stages.
+template <bool CONV, int BN>
+int launch_pipe_s(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, void* C, int ldc, int M, int N,
+                  int K, const float* bias, int relu, int out_mode, int* err, ConvShape cs, cudaStream_t s) {
+    if ((K + GK - 1) / GK <= 8)
+        return launch_pipe<CONV, BN, 2>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
+    return launch_pipe<CONV, BN, 4>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
 }
 
 template <bool CONV>
 int launch_pipe_n(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, void* C, int ldc, int M, int N,
                   int K, const float* bias, int relu, int out_mode, int* err, ConvShape cs, cudaStream_t s) {
-    if (N <= 32) return launch_pipe<CONV, 32>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
-    if (N <= 64) return launch_pipe<CONV, 64>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
-    return launch_pipe<CONV, 128>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
+    if (N <= 32) return launch_pipe_s<CONV, 32>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
+    if (N <= 64) return launch_pipe_s<CONV, 64>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
+    return launch_pipe_s<CONV, 128>(A, lda, B, ldb, C, ldc, M, N, K, bias, relu, out_mode, err, cs, s);
 }
 
 inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }

@@ -391,6 +391,10 @@ class IcePhysics:
         k = 0
         prev = 1.0
         rel = 1.0
+        if tol is not None and n_max <= 0:
+            # no cycles (max_vcycles=0): the finish alone, from the current state
+            rel = self.residual_norm() / r0 if r0 > 0 else 0.0
+            prev = rel
         stalled = False
         good = self._good_state() if tol is not None else None
         while k < n_max:
