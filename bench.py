@@ -204,7 +204,7 @@ def fast_settings():
                           n_smooth=6, n_coarse=20)
 
 
-FAST_KW = dict(finish_anderson=5, finish_fp32=True, finish_newton=2, finish_step=1.0, finish_linear="after",
+FAST_KW = dict(finish_anderson=3, finish_fp32=True, finish_newton=2, finish_step=1.0, finish_linear="after",
                finish_fas_until=2e-4, finish_fas_patience=8,
                newton=True, newton_start=1e-2, newton_after=200, newton_min_gain=4.0, newton_local=2,
                newton_max_steps=6)
@@ -212,10 +212,10 @@ FAST_KW = dict(finish_anderson=5, finish_fp32=True, finish_newton=2, finish_step
 TIGHT_KW = {k: v for k, v in FAST_KW.items() if not k.startswith("newton")}
 # the fast path's smoother and finishing rule in FP64 (no FP32 correction stages; the
 # Newton-Krylov finish on the FP64 hierarchy)
-FP64_FAST_KW = dict(finish_anderson=5, finish_newton=2, finish_step=1.0,
+FP64_FAST_KW = dict(finish_anderson=3, finish_newton=2, finish_step=1.0,
                     **{k: v for k, v in FAST_KW.items() if k.startswith("newton")})
 FAST_PATH = ("mixed FAS, full-step local Newton x2, finishing sweeps FP32 (FAS form, then linearised) / FP64 + "
-             "Anderson(5); after 200 sweeps a Newton-Krylov finish (FGMRES, linear multigrid V-cycle "
+             "Anderson(3); after 200 sweeps a Newton-Krylov finish (FGMRES, linear multigrid V-cycle "
              "preconditioner) while its steps gain >= 4x")
 
 
