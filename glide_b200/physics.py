@@ -674,22 +674,10 @@ class IcePhysics:
         rH = g.r_H
         fb = (Hm + rH - torch.sqrt(Hm * Hm + rH * rH)).abs().flatten()
         k = int(torch.argmax(fb).item())
-        H = float(g.H.flatten()[k])
-        bed = float(g.bed.flatten()[k])
-        fH = float(g.f_H.flatten()[k])
-        r = float(rH.flatten()[k])
-        dt, c = float(g.dt), self.calving_rate
-        z = max(min(self.gl_sigmoid_c * (bed + RHO_ICE / 1000.0 * H), 20.0), -20.0)
-        gnd = 1.0 / (1.0 + math.exp(-z))
-        S = fH - (r - H / dt - c * (1.0 - gnd) * H + fH)   # f_H - D
-        flot = -bed / (RHO_ICE / 1000.0)
-        if gnd > 0.5:
-            H_new = S / (1.0 / dt + c)
-            ok = H_new < flot
-        else:
-            H_new = S * dt
-            ok = H_new > flot
-        if not (ok and math.isfinite(H_new) and H_new > self.thklim):
+        H_new = other_mass_root(float(g.H.flatten()[k]), float(g.bed.flatten()[k]), float(g.f_H.flatten()[k]),
+                                float(rH.flatten()[k]), float(g.dt), self.calving_rate, self.gl_sigmoid_c,
+                                self.thklim)
+        if H_new is None:
             return False
         g.H.view(-1)[k] = H_new
         return True
@@ -916,6 +904,31 @@ class IcePhysics:
             self._nk.release()
         if self._ak is not None:
             self._ak.release()
+
+
+def other_mass_root(H, bed, f_H, r_H, dt, calving_rate, sig_c, thklim):
+    """The other root of one cell's mass balance with its net outflow fixed.
+
+    r_H(H) = H/dt + c (1 - g(H)) H + D - f_H (glide/cuda/flux.cu:187-211,
+    g the grounding sigmoid of bed + 0.917 H); D is taken from the cell's
+    residual r_H at its thickness H.  Grounded (g > 1/2): the floating root
+    (f_H - D) / (1/dt + c), if it lies below the flotation thickness;
+    floating: the grounded root (f_H - D) dt, if it lies above it.  None when
+    that root does not exist or is not above thklim."""
+    rr = RHO_ICE / 1000.0
+    z = max(min(sig_c * (bed + rr * H), 20.0), -20.0)
+    gnd = 1.0 / (1.0 + math.exp(-z))
+    S = f_H - (r_H - H / dt - calving_rate * (1.0 - gnd) * H + f_H)   # f_H - D
+    flot = -bed / rr
+    if gnd > 0.5:
+        H_new = S / (1.0 / dt + calving_rate)
+        ok = H_new < flot
+    else:
+        H_new = S * dt
+        ok = H_new > flot
+    if not (ok and math.isfinite(H_new) and H_new > thklim):
+        return None
+    return H_new
 
 
 # ---------------------------------------------------------------------------
